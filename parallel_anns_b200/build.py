@@ -1,0 +1,59 @@
+"""Build recipe of the native library: nvcc for sm_100a, in-tree.
+
+``python -m parallel_anns_b200.build`` (or ``build()``) compiles
+``csrc/*.cu`` into ``parallel_anns_b200/libpanns_b200.so``, which exports the
+C ABI declared in ``include/panns_b200.h``.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+SO = os.path.join(PKG, "libpanns_b200.so")
+SOURCES = [os.path.join(PKG, "csrc", "panns_abi.cu")]
+DEPS = SOURCES + [
+    os.path.join(PKG, "csrc", "search_kernel.cuh"),
+    os.path.join(ROOT, "include", "panns_b200.h"),
+]
+
+NVCC_FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-O3", "-lineinfo", "-std=c++17",
+    "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
+    "-shared",
+]
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def up_to_date() -> bool:
+    if not os.path.exists(SO):
+        return False
+    t = os.path.getmtime(SO)
+    return all(os.path.getmtime(p) <= t for p in DEPS if os.path.exists(p))
+
+
+def build(force: bool = False, verbose: bool = False, extra=None) -> str:
+    if not force and up_to_date():
+        return SO
+    cmd = [nvcc()] + NVCC_FLAGS + (extra or []) + ["-o", SO + ".tmp"] + SOURCES + ["-lcudart"]
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    subprocess.run(cmd, check=True, cwd=PKG)
+    os.replace(SO + ".tmp", SO)
+    return SO
+
+
+if __name__ == "__main__":
+    v = "-v" in sys.argv
+    extra = ["-Xptxas", "-v"] if "--ptxas" in sys.argv else None
+    print(build(force=True, verbose=v, extra=extra))

@@ -1,0 +1,771 @@
+// C ABI of panns_b200 (declared in include/panns_b200.h): loaders, the HBM
+// layout of the base vectors and the graph, init-id generation, the batched
+// search launch and recall. Host code is C++; the hot path is search_kernel.cuh.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/panns_b200.h"
+#include "search_kernel.cuh"
+
+using namespace panns;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg) {
+    g_err = msg;
+    return code;
+}
+
+#define CU(call)                                                                       \
+    do {                                                                               \
+        cudaError_t e_ = (call);                                                       \
+        if (e_ != cudaSuccess)                                                         \
+            return fail(PANNS_ECUDA, std::string(#call ": ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+// Chain-major padding: the reference's lane accumulator c visits the terms
+// c, c+8, c+16, ... (after the last 8 elements when d % 16 == 8). Term k of
+// chain c is stored at float (8 * (k / 4) + c) * 4 + k % 4 of the padded row.
+__host__ __device__ inline int chain_term_element(int d, int c, int k) {
+    const int DR = d % 16, DD = d - DR;
+    const int nterms = d / 8;
+    if (k >= nterms) return -1;
+    if (DR) return k == 0 ? DD + c : c + 8 * (k - 1);
+    return c + 8 * k;
+}
+
+__global__ void permute_rows_kernel(const float *__restrict__ raw, float *__restrict__ out,
+                                    uint64_t rows, int d, int dpad) {
+    const uint64_t total = rows * (uint64_t) dpad;
+    for (uint64_t t = blockIdx.x * (uint64_t) blockDim.x + threadIdx.x; t < total;
+         t += (uint64_t) gridDim.x * blockDim.x) {
+        const uint64_t r = t / dpad;
+        const int p = (int) (t % dpad);
+        const int chunk = p >> 2, i = chunk >> 3, c = chunk & 7;
+        const int k = 4 * i + (p & 3);
+        const int e = chain_term_element(d, c, k);
+        out[t] = e >= 0 ? raw[r * d + e] : 0.0f;
+    }
+}
+
+// ||v||^2 from the chain-major rows: lane c = FMA chain over its terms, then
+// the lanes summed 0..7 (core/Searching.202102022027.PSS_v5.dist_thresh.profiling.cpp:294-335).
+__global__ void norms_kernel(const float *__restrict__ vec, float *__restrict__ norms, uint32_t n,
+                             int dpad) {
+    const int CL = dpad / 32;
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        const float *row = vec + (size_t) v * dpad;
+        float acc[8];
+        for (int c = 0; c < 8; ++c) {
+            float a = 0.0f;
+            for (int i = 0; i < CL; ++i)
+                for (int j = 0; j < 4; ++j) {
+                    const float x = row[(8 * i + c) * 4 + j];
+                    a = __fmaf_rn(x, x, a);
+                }
+            acc[c] = a;
+        }
+        float s = acc[0];
+        for (int c = 1; c < 8; ++c) s = __fadd_rn(s, acc[c]);
+        norms[v] = s;
+    }
+}
+
+template <typename T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    cudaError_t ensure(size_t count) {
+        if (count <= n && p) return cudaSuccess;
+        release();
+        cudaError_t e = cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T));
+        if (e == cudaSuccess) n = count;
+        else p = nullptr;
+        return e;
+    }
+};
+
+}  // namespace
+
+struct panns_index {
+    int device = 0;
+    int num_sms = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // base vectors
+    uint32_t n = 0, d = 0, dpad = 0, storage = 0;
+    DevBuf<float> vec, norms;
+    // graph
+    uint32_t width = 0, entry = 0, gn = 0;
+    std::vector<uint64_t> off;
+    std::vector<uint32_t> nbrs;
+    DevBuf<uint32_t> head, ovf;
+    DevBuf<uint64_t> ovf_off;
+    // queries
+    uint32_t nq = 0, qd = 0;
+    DevBuf<float> queries;  // chain-major
+    // scratch
+    DevBuf<float> raw;      // staging for permutation
+    DevBuf<uint32_t> visited, dirty, counter, error, init, out;
+    DevBuf<uint4> stats;
+    uint32_t vis_slots = 0, vis_words = 0, dirty_cap = 0;
+    std::vector<uint4> h_stats;
+};
+
+extern "C" {
+
+const char *panns_last_error(void) { return g_err.c_str(); }
+uint32_t panns_version(void) { return (1u << 16) | 0u; }
+
+int panns_open(panns_index **out, int device) {
+    if (!out) return fail(PANNS_EINVAL, "panns_open: out is NULL");
+    *out = nullptr;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0)
+        return fail(PANNS_ECUDA, std::string("no CUDA device: ") + cudaGetErrorString(e));
+    if (device < 0 || device >= count) return fail(PANNS_EINVAL, "panns_open: bad device index");
+    CU(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    CU(cudaGetDeviceProperties(&prop, device));
+    if (prop.major < 10)
+        return fail(PANNS_ECUDA, "panns_b200 is built for sm_100a (B200); found sm_" +
+                                     std::to_string(prop.major) + std::to_string(prop.minor));
+    std::unique_ptr<panns_index> h(new panns_index());
+    h->device = device;
+    h->num_sms = prop.multiProcessorCount;
+    CU(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    CU(cudaEventCreate(&h->ev0));
+    CU(cudaEventCreate(&h->ev1));
+    *out = h.release();
+    return PANNS_OK;
+}
+
+int panns_close(panns_index *h) {
+    if (!h) return PANNS_OK;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return PANNS_OK;
+}
+
+static int upload_chain_major(panns_index *h, const float *rows, uint64_t count, uint32_t d,
+                              DevBuf<float> &dst) {
+    const uint32_t dpad = ((d + 31) / 32) * 32;
+    CU(h->raw.ensure(count * d));
+    CU(dst.ensure(count * dpad));
+    CU(cudaMemcpyAsync(h->raw.p, rows, count * d * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    const uint64_t total = count * dpad;
+    const int blocks = (int) std::min<uint64_t>((total + 255) / 256, (uint64_t) h->num_sms * 32);
+    permute_rows_kernel<<<std::max(blocks, 1), 256, 0, h->stream>>>(h->raw.p, dst.p, count, (int) d,
+                                                                   (int) dpad);
+    CU(cudaGetLastError());
+    return PANNS_OK;
+}
+
+int panns_set_base(panns_index *h, const float *data, uint32_t n, uint32_t d, uint32_t storage) {
+    if (!h || !data) return fail(PANNS_EINVAL, "panns_set_base: NULL argument");
+    if (n == 0 || d == 0) return fail(PANNS_EINVAL, "panns_set_base: empty base");
+    if (d % 8) return fail(PANNS_EINVAL, "panns_set_base: d must be a multiple of 8");
+    if (d > 256) return fail(PANNS_EINVAL, "panns_set_base: d > 256 is not supported");
+    if (n > 0x7fffffffu) return fail(PANNS_EINVAL, "panns_set_base: n must be < 2^31");
+    if (storage != PANNS_STORE_FP32)
+        return fail(PANNS_EINVAL, "panns_set_base: only FP32 storage is available in this build");
+    if (h->qd && h->qd != d) return fail(PANNS_EINVAL, "panns_set_base: dimension differs from the queries");
+    CU(cudaSetDevice(h->device));
+    int rc = upload_chain_major(h, data, n, d, h->vec);
+    if (rc) return rc;
+    h->n = n;
+    h->d = d;
+    h->dpad = ((d + 31) / 32) * 32;
+    h->storage = storage;
+    CU(h->norms.ensure(n));
+    const int blocks = std::max(1, (int) std::min<uint32_t>((n + 255) / 256, h->num_sms * 32u));
+    norms_kernel<<<blocks, 256, 0, h->stream>>>(h->vec.p, h->norms.p, n, (int) h->dpad);
+    CU(cudaGetLastError());
+    CU(cudaStreamSynchronize(h->stream));
+    h->raw.release();
+    return PANNS_OK;
+}
+
+static int read_fvecs(const char *path, std::vector<float> &v, uint32_t &n, uint32_t &d) {
+    FILE *f = fopen(path, "rb");
+    if (!f) return fail(PANNS_EIO, std::string("cannot open ") + path);
+    uint32_t dim = 0;
+    if (fread(&dim, 4, 1, f) != 1) {
+        fclose(f);
+        return fail(PANNS_EIO, std::string("empty fvecs file ") + path);
+    }
+    fseek(f, 0, SEEK_END);
+    const uint64_t sz = (uint64_t) ftell(f);
+    fseek(f, 0, SEEK_SET);
+    if (dim == 0 || sz % (4ull * (dim + 1))) {
+        fclose(f);
+        return fail(PANNS_EIO, std::string("fvecs size is not a whole number of rows: ") + path);
+    }
+    const uint64_t rows = sz / (4ull * (dim + 1));
+    if (rows > 0x7fffffffull) {
+        fclose(f);
+        return fail(PANNS_EIO, "fvecs: too many rows");
+    }
+    v.resize(rows * dim);
+    std::vector<uint32_t> rec(dim + 1);
+    for (uint64_t i = 0; i < rows; ++i) {
+        if (fread(rec.data(), 4, dim + 1, f) != dim + 1 || rec[0] != dim) {
+            fclose(f);
+            return fail(PANNS_EIO, std::string("fvecs row ") + std::to_string(i) + " is malformed");
+        }
+        memcpy(v.data() + i * dim, rec.data() + 1, 4ull * dim);
+    }
+    fclose(f);
+    n = (uint32_t) rows;
+    d = dim;
+    return PANNS_OK;
+}
+
+int panns_load_fvecs_base(panns_index *h, const char *path, uint32_t storage) {
+    if (!h || !path) return fail(PANNS_EINVAL, "panns_load_fvecs_base: NULL argument");
+    std::vector<float> v;
+    uint32_t n = 0, d = 0;
+    int rc = read_fvecs(path, v, n, d);
+    if (rc) return rc;
+    return panns_set_base(h, v.data(), n, d, storage);
+}
+
+int panns_set_queries(panns_index *h, const float *queries, uint32_t nq, uint32_t d) {
+    if (!h || (!queries && nq)) return fail(PANNS_EINVAL, "panns_set_queries: NULL argument");
+    if (d % 8 || d == 0 || d > 256) return fail(PANNS_EINVAL, "panns_set_queries: bad dimension");
+    if (h->d && d != h->d) return fail(PANNS_EINVAL, "panns_set_queries: dimension differs from the base");
+    CU(cudaSetDevice(h->device));
+    if (nq) {
+        int rc = upload_chain_major(h, queries, nq, d, h->queries);
+        if (rc) return rc;
+        CU(cudaStreamSynchronize(h->stream));
+        h->raw.release();
+    }
+    h->nq = nq;
+    h->qd = d;
+    return PANNS_OK;
+}
+
+int panns_load_fvecs_queries(panns_index *h, const char *path) {
+    if (!h || !path) return fail(PANNS_EINVAL, "panns_load_fvecs_queries: NULL argument");
+    std::vector<float> v;
+    uint32_t n = 0, d = 0;
+    int rc = read_fvecs(path, v, n, d);
+    if (rc) return rc;
+    return panns_set_queries(h, v.data(), n, d);
+}
+
+int panns_set_graph(panns_index *h, uint32_t width, uint32_t entry, const uint64_t *offsets,
+                    const uint32_t *nbrs, uint32_t n) {
+    if (!h || !offsets || (!nbrs && offsets[n])) return fail(PANNS_EINVAL, "panns_set_graph: NULL argument");
+    if (n == 0) return fail(PANNS_EINVAL, "panns_set_graph: empty graph");
+    if (h->n && n != h->n)
+        return fail(PANNS_EINVAL, "panns_set_graph: graph has " + std::to_string(n) +
+                                      " vertices, the base has " + std::to_string(h->n));
+    if (entry >= n) return fail(PANNS_EINVAL, "panns_set_graph: entry vertex out of range");
+    if (offsets[0] != 0) return fail(PANNS_EINVAL, "panns_set_graph: offsets[0] must be 0");
+    for (uint32_t v = 0; v < n; ++v)
+        if (offsets[v + 1] < offsets[v]) return fail(PANNS_EINVAL, "panns_set_graph: offsets not monotone");
+    const uint64_t E = offsets[n];
+    for (uint64_t e = 0; e < E; ++e)
+        if (nbrs[e] >= n)
+            return fail(PANNS_EINVAL, "panns_set_graph: neighbour id " + std::to_string(nbrs[e]) +
+                                          " >= N");
+    CU(cudaSetDevice(h->device));
+    h->off.assign(offsets, offsets + n + 1);
+    h->nbrs.assign(nbrs, nbrs + E);
+    std::vector<uint32_t> head((size_t) n * kHeadWords, 0u);
+    std::vector<uint64_t> ovf_off(n, 0);
+    std::vector<uint32_t> ovf;
+    for (uint32_t v = 0; v < n; ++v) {
+        const uint64_t deg = offsets[v + 1] - offsets[v];
+        uint32_t *row = head.data() + (size_t) v * kHeadWords;
+        row[0] = (uint32_t) deg;
+        const uint64_t h1 = std::min<uint64_t>(deg, kHeadNbrs);
+        for (uint64_t s = 0; s < h1; ++s) row[1 + s] = nbrs[offsets[v] + s];
+        if (deg > (uint64_t) kHeadNbrs) {
+            ovf_off[v] = ovf.size();
+            ovf.insert(ovf.end(), nbrs + offsets[v] + kHeadNbrs, nbrs + offsets[v + 1]);
+        }
+    }
+    CU(h->head.ensure(head.size()));
+    CU(h->ovf_off.ensure(n));
+    CU(h->ovf.ensure(std::max<size_t>(ovf.size(), 1)));
+    CU(cudaMemcpyAsync(h->head.p, head.data(), head.size() * 4, cudaMemcpyHostToDevice, h->stream));
+    CU(cudaMemcpyAsync(h->ovf_off.p, ovf_off.data(), n * 8ull, cudaMemcpyHostToDevice, h->stream));
+    if (!ovf.empty())
+        CU(cudaMemcpyAsync(h->ovf.p, ovf.data(), ovf.size() * 4, cudaMemcpyHostToDevice, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    h->width = width;
+    h->entry = entry;
+    h->gn = n;
+    return PANNS_OK;
+}
+
+int panns_load_nsg(panns_index *h, const char *path) {
+    if (!h || !path) return fail(PANNS_EINVAL, "panns_load_nsg: NULL argument");
+    FILE *f = fopen(path, "rb");
+    if (!f) return fail(PANNS_EIO, std::string("cannot open ") + path);
+    uint32_t hdr[2];
+    if (fread(hdr, 4, 2, f) != 2) {
+        fclose(f);
+        return fail(PANNS_EIO, std::string("truncated .nsg header: ") + path);
+    }
+    std::vector<uint64_t> off(1, 0);
+    std::vector<uint32_t> nb;
+    for (;;) {
+        uint32_t deg;
+        if (fread(&deg, 4, 1, f) != 1) break;
+        const size_t at = nb.size();
+        nb.resize(at + deg);
+        if (deg && fread(nb.data() + at, 4, deg, f) != deg) {
+            fclose(f);
+            return fail(PANNS_EIO, std::string("truncated .nsg row ") + std::to_string(off.size() - 1) +
+                                       ": " + path);
+        }
+        off.push_back(nb.size());
+    }
+    fclose(f);
+    const uint32_t n = (uint32_t) (off.size() - 1);
+    if (n == 0) return fail(PANNS_EIO, std::string(".nsg has no vertices: ") + path);
+    return panns_set_graph(h, hdr[0], hdr[1], off.data(), nb.data(), n);
+}
+
+int panns_info(const panns_index *h, uint32_t *n, uint32_t *d, uint32_t *nq, uint32_t *width,
+               uint32_t *entry) {
+    if (!h) return fail(PANNS_EINVAL, "panns_info: NULL handle");
+    if (n) *n = h->n ? h->n : h->gn;
+    if (d) *d = h->d;
+    if (nq) *nq = h->nq;
+    if (width) *width = h->width;
+    if (entry) *entry = h->entry;
+    return PANNS_OK;
+}
+
+int panns_prepare_init_ids(const panns_index *h, uint32_t L, uint32_t *out) {
+    if (!h || !out) return fail(PANNS_EINVAL, "panns_prepare_init_ids: NULL argument");
+    if (!h->gn) return fail(PANNS_ESTATE, "panns_prepare_init_ids: no graph loaded");
+    const uint32_t n = h->gn;
+    if (L == 0 || L > n) return fail(PANNS_EINVAL, "panns_prepare_init_ids: need 0 < L <= N");
+    std::vector<uint8_t> sel(n, 0);
+    uint32_t end = 0;
+    for (uint64_t e = h->off[h->entry]; e < h->off[h->entry + 1] && end < L; ++e) {
+        const uint32_t v = h->nbrs[e];
+        if (sel[v]) continue;
+        sel[v] = 1;
+        out[end++] = v;
+    }
+    uint32_t t = h->entry + 1;
+    while (end < L) {
+        if (t == n) t = 0;
+        const uint32_t v = t++;
+        if (sel[v]) continue;
+        sel[v] = 1;
+        out[end++] = v;
+    }
+    return PANNS_OK;
+}
+
+// glibc rand(): the additive feedback generator r[i] = r[i-3] + r[i-31]
+// (mod 2^32) over a 31-word table seeded with the Park-Miller sequence
+// 16807 * r mod (2^31 - 1) from `seed`, first 310 outputs discarded, each
+// output (r >> 1). State layout: table[31], front index, rear index.
+static int32_t rand_next(int32_t *st) {
+    int32_t *tbl = st;
+    int32_t &fi = st[31], &ri = st[32];
+    const uint32_t val = (uint32_t) tbl[fi] + (uint32_t) tbl[ri];
+    tbl[fi] = (int32_t) val;
+    if (++fi >= 31) {
+        fi = 0;
+        ++ri;
+    } else if (++ri >= 31) {
+        ri = 0;
+    }
+    return (int32_t) (val >> 1);
+}
+
+int panns_rand_seed(int32_t *st, uint32_t seed) {
+    if (!st) return fail(PANNS_EINVAL, "panns_rand_seed: NULL state");
+    if (seed == 0) seed = 1;
+    st[0] = (int32_t) seed;
+    for (int i = 1; i < 31; ++i) {
+        const int64_t hi = st[i - 1] / 127773, lo = st[i - 1] % 127773;
+        int64_t w = 16807 * lo - 2836 * hi;
+        if (w < 0) w += 2147483647;
+        st[i] = (int32_t) w;
+    }
+    st[31] = 3;
+    st[32] = 0;
+    for (int i = 0; i < 310; ++i) rand_next(st);
+    return PANNS_OK;
+}
+
+int panns_efanna_init_ids(const panns_index *h, uint32_t L, uint32_t nq, int32_t *st, uint32_t *out) {
+    if (!h || !out || !st) return fail(PANNS_EINVAL, "panns_efanna_init_ids: NULL argument");
+    if (!h->gn) return fail(PANNS_ESTATE, "panns_efanna_init_ids: no graph loaded");
+    const uint32_t n = h->gn;
+    if (L == 0 || L > n) return fail(PANNS_EINVAL, "panns_efanna_init_ids: need 0 < L <= N");
+    std::vector<uint8_t> flags(n, 0);
+    const uint64_t e0 = h->off[h->entry], deg = h->off[h->entry + 1] - e0;
+    for (uint32_t q = 0; q < nq; ++q) {
+        uint32_t *ids = out + (size_t) q * L;
+        uint32_t t = 0;
+        for (; t < L && t < deg; ++t) {
+            ids[t] = h->nbrs[e0 + t];
+            flags[ids[t]] = 1;
+        }
+        while (t < L) {
+            const uint32_t id = (uint32_t) rand_next(st) % n;
+            if (flags[id]) continue;
+            flags[id] = 1;
+            ids[t++] = id;
+        }
+        for (uint32_t i = 0; i < L; ++i) flags[ids[i]] = 0;
+    }
+    return PANNS_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Search launch
+// ---------------------------------------------------------------------------
+namespace {
+
+template <int KIND, int ORDER>
+const void *pick_kernel(int CL) {
+    switch (CL) {
+        case 1: return (const void *) search_kernel<KIND, ORDER, 1>;
+        case 2: return (const void *) search_kernel<KIND, ORDER, 2>;
+        case 3: return (const void *) search_kernel<KIND, ORDER, 3>;
+        case 4: return (const void *) search_kernel<KIND, ORDER, 4>;
+        case 5: return (const void *) search_kernel<KIND, ORDER, 5>;
+        case 6: return (const void *) search_kernel<KIND, ORDER, 6>;
+        case 7: return (const void *) search_kernel<KIND, ORDER, 7>;
+        case 8: return (const void *) search_kernel<KIND, ORDER, 8>;
+    }
+    return nullptr;
+}
+
+const void *kernel_for(uint32_t kind, uint32_t order, int CL) {
+    if (kind == KIND_IP)
+        return order == ORDER_PANNS ? pick_kernel<KIND_IP, ORDER_PANNS>(CL)
+                                    : pick_kernel<KIND_IP, ORDER_EFANNA>(CL);
+    return order == ORDER_PANNS ? pick_kernel<KIND_L2, ORDER_PANNS>(CL)
+                                : pick_kernel<KIND_L2, ORDER_EFANNA>(CL);
+}
+
+int check_params(const panns_index *h, const panns_search_params *p) {
+    if (!p) return fail(PANNS_EINVAL, "search: NULL params");
+    if (!h->n || !h->vec.p) return fail(PANNS_ESTATE, "search: no base vectors loaded");
+    if (!h->gn || !h->head.p) return fail(PANNS_ESTATE, "search: no graph loaded");
+    if (h->gn != h->n) return fail(PANNS_ESTATE, "search: graph and base sizes differ");
+    if (p->mode > PANNS_MODE_EFANNA) return fail(PANNS_EINVAL, "search: unknown mode");
+    if (p->distance > PANNS_DIST_L2) return fail(PANNS_EINVAL, "search: unknown distance");
+    if (p->L == 0 || p->L > h->n) return fail(PANNS_EINVAL, "search: need 0 < L <= N");
+    if (p->K == 0 || p->K > p->L) return fail(PANNS_EINVAL, "search: need 0 < K <= L");
+    if (p->L > 8192) return fail(PANNS_EINVAL, "search: L > 8192 is not supported");
+    if (p->mode == PANNS_MODE_TOP_M && (p->M == 0 || p->M > (uint32_t) kMaxM))
+        return fail(PANNS_EINVAL, "search: TOP_M needs 1 <= M <= 64");
+    if (p->mode == PANNS_MODE_PSS_V5) {
+        if (p->T == 0 || p->X == 0) return fail(PANNS_EINVAL, "search: PSS_V5 needs T >= 1 and X >= 1");
+        if (p->T > 1) return fail(PANNS_EINVAL, "search: PSS_V5 with T > 1 is not available in this build");
+    }
+    if (p->warps_per_block > 8) return fail(PANNS_EINVAL, "search: warps_per_block must be <= 8");
+    if (p->flags) return fail(PANNS_EINVAL, "search: flags must be 0");
+    return PANNS_OK;
+}
+
+}  // namespace
+
+// Launch the search for nq chain-major device queries; everything enqueued on `stream`.
+static int launch_search(panns_index *h, const panns_search_params *p, const float *d_queries_cm,
+                         uint32_t nq, const uint32_t *h_init, uint32_t init_count,
+                         uint32_t init_stride, uint32_t *d_out, uint4 *d_stats,
+                         cudaStream_t stream, bool time_it) {
+    const int CL = (int) (h->dpad / 32);
+    const uint32_t order = p->mode == PANNS_MODE_EFANNA ? ORDER_EFANNA : ORDER_PANNS;
+    const uint32_t kind = p->distance == PANNS_DIST_L2 ? KIND_L2 : KIND_IP;
+    const void *kern = kernel_for(kind, order, CL);
+    if (!kern) return fail(PANNS_EINVAL, "search: unsupported dimension");
+    const uint32_t M = p->mode == PANNS_MODE_TOP_M ? p->M : 1u;
+    const uint32_t qcap = ((p->L + 31) / 32) * 32;
+    const uint32_t wpb = p->warps_per_block ? p->warps_per_block : 4u;
+    const size_t smem = (size_t) wpb * warp_smem_bytes(qcap);
+    CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+    int per_sm = 0;
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (int) wpb * 32, smem));
+    if (per_sm < 1) return fail(PANNS_EINVAL, "search: L too large for shared memory");
+    uint32_t blocks = (uint32_t) per_sm * (uint32_t) h->num_sms;
+    const uint32_t need_blocks = (nq + wpb - 1) / wpb;
+    blocks = std::max(1u, std::min(blocks, need_blocks));
+    const uint32_t slots = blocks * wpb;
+    // Per-slot visited bitsets (bounded to 16 GiB) and dirty-word lists.
+    const uint32_t vis_words = (h->n + 31) / 32;
+    const uint32_t dirty_cap = 8192;
+    if ((uint64_t) slots * vis_words * 4 > (16ull << 30)) {
+        const uint32_t max_slots = (uint32_t) ((16ull << 30) / (vis_words * 4ull));
+        blocks = std::max(1u, max_slots / wpb);
+    }
+    const uint32_t nslots = blocks * wpb;
+    if (h->vis_slots < nslots || h->vis_words != vis_words) {
+        CU(h->visited.ensure((size_t) nslots * vis_words));
+        CU(cudaMemsetAsync(h->visited.p, 0, (size_t) nslots * vis_words * 4, stream));
+        CU(h->dirty.ensure((size_t) nslots * dirty_cap));
+        h->vis_slots = nslots;
+        h->vis_words = vis_words;
+    }
+    CU(h->counter.ensure(1));
+    CU(h->error.ensure(1));
+    CU(h->init.ensure(std::max<size_t>(init_count, 1)));
+    CU(cudaMemcpyAsync(h->init.p, h_init, (size_t) init_count * 4, cudaMemcpyHostToDevice, stream));
+    CU(cudaMemsetAsync(h->counter.p, 0, 4, stream));
+    CU(cudaMemsetAsync(h->error.p, 0, 4, stream));
+    SearchArgs a;
+    a.vec = reinterpret_cast<const float4 *>(h->vec.p);
+    a.norms = h->norms.p;
+    a.head = h->head.p;
+    a.ovf_off = h->ovf_off.p;
+    a.ovf = h->ovf.p;
+    a.n = h->n;
+    a.queries = reinterpret_cast<const float4 *>(d_queries_cm);
+    a.nq = nq;
+    a.init_ids = h->init.p;
+    a.init_stride = init_stride;
+    a.K = p->K;
+    a.L = p->L;
+    a.M = M;
+    a.out_ids = d_out;
+    a.out_stats = d_stats;
+    a.visited = h->visited.p;
+    a.vis_words = vis_words;
+    a.dirty = h->dirty.p;
+    a.dirty_cap = dirty_cap;
+    a.counter = h->counter.p;
+    a.error = h->error.p;
+    a.queue_cap = qcap;
+    void *args[] = {&a};
+    if (time_it) CU(cudaEventRecord(h->ev0, stream));
+    CU(cudaLaunchKernel(kern, dim3(blocks), dim3(wpb * 32), args, smem, stream));
+    if (time_it) CU(cudaEventRecord(h->ev1, stream));
+    return PANNS_OK;
+}
+
+static int resolve_init(panns_index *h, const panns_search_params *p, const uint32_t *init_ids,
+                        uint32_t nq, std::vector<uint32_t> &buf, const uint32_t *&ids,
+                        uint32_t &count, uint32_t &stride) {
+    const uint32_t L = p->L;
+    if (p->mode == PANNS_MODE_EFANNA) {
+        stride = L;
+        count = nq * L;
+        if (init_ids) {
+            ids = init_ids;
+        } else {
+            int32_t st[40];
+            panns_rand_seed(st, 1);
+            buf.resize((size_t) nq * L);
+            int rc = panns_efanna_init_ids(h, L, nq, st, buf.data());
+            if (rc) return rc;
+            ids = buf.data();
+        }
+    } else {
+        stride = 0;
+        count = L;
+        if (init_ids) {
+            ids = init_ids;
+        } else {
+            buf.resize(L);
+            int rc = panns_prepare_init_ids(h, L, buf.data());
+            if (rc) return rc;
+            ids = buf.data();
+        }
+    }
+    // Init ids must be valid, distinct vertices (per query).
+    const uint32_t groups = stride ? nq : 1;
+    std::vector<uint8_t> seen(h->n, 0);
+    for (uint32_t g = 0; g < groups; ++g) {
+        const uint32_t *x = ids + (size_t) g * L;
+        for (uint32_t i = 0; i < L; ++i) {
+            if (x[i] >= h->n) return fail(PANNS_EINVAL, "search: init id out of range");
+            if (seen[x[i]]) return fail(PANNS_EINVAL, "search: duplicate init id");
+            seen[x[i]] = 1;
+        }
+        for (uint32_t i = 0; i < L; ++i) seen[x[i]] = 0;
+    }
+    return PANNS_OK;
+}
+
+static int finish(panns_index *h, uint32_t nq, uint32_t K, uint32_t *out_ids, panns_stats *stats,
+                  double t0_ms) {
+    h->h_stats.resize(nq);
+    uint32_t err = 0;
+    CU(cudaMemcpyAsync(out_ids, h->out.p, (size_t) nq * K * 4, cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaMemcpyAsync(h->h_stats.data(), h->stats.p, (size_t) nq * sizeof(uint4), cudaMemcpyDeviceToHost,
+                       h->stream));
+    CU(cudaMemcpyAsync(&err, h->error.p, 4, cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    if (err & ERR_BAD_ID) return fail(PANNS_EDEVICE, "search: the graph holds a neighbour id >= N");
+    if (err & ERR_BAD_INIT) return fail(PANNS_EDEVICE, "search: init id >= N");
+    if (stats) {
+        memset(stats, 0, sizeof(*stats));
+        for (const uint4 &s : h->h_stats) {
+            stats->n_dist += s.x;
+            stats->n_expand += s.y;
+            stats->n_edges += s.z;
+            stats->n_iter += s.w;
+        }
+        float ms = 0.f;
+        CU(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+        stats->kernel_ms = ms;
+        const double t1 = std::chrono::duration<double, std::milli>(
+                              std::chrono::steady_clock::now().time_since_epoch()).count();
+        stats->total_ms = t1 - t0_ms;
+    }
+    return PANNS_OK;
+}
+
+static double now_ms() {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch())
+        .count();
+}
+
+extern "C" {
+
+int panns_search(panns_index *h, const panns_search_params *p, const uint32_t *init_ids,
+                 uint32_t q_begin, uint32_t nq, uint32_t *out_ids, panns_stats *stats) {
+    if (!h) return fail(PANNS_EINVAL, "panns_search: NULL handle");
+    const double t0 = now_ms();
+    int rc = check_params(h, p);
+    if (rc) return rc;
+    if (!out_ids && nq) return fail(PANNS_EINVAL, "panns_search: NULL out_ids");
+    if ((uint64_t) q_begin + nq > h->nq) return fail(PANNS_EINVAL, "panns_search: query range out of bounds");
+    if (nq == 0) {
+        if (stats) memset(stats, 0, sizeof(*stats));
+        return PANNS_OK;
+    }
+    CU(cudaSetDevice(h->device));
+    std::vector<uint32_t> buf;
+    const uint32_t *ids = nullptr;
+    uint32_t count = 0, stride = 0;
+    rc = resolve_init(h, p, init_ids, nq, buf, ids, count, stride);
+    if (rc) return rc;
+    CU(h->out.ensure((size_t) nq * p->K));
+    CU(h->stats.ensure(nq));
+    rc = launch_search(h, p, h->queries.p + (size_t) q_begin * h->dpad, nq, ids, count, stride, h->out.p,
+                       h->stats.p, h->stream, true);
+    if (rc) return rc;
+    return finish(h, nq, p->K, out_ids, stats, t0);
+}
+
+int panns_search_host(panns_index *h, const panns_search_params *p, const float *queries, uint32_t nq,
+                      const uint32_t *init_ids, uint32_t *out_ids, panns_stats *stats) {
+    if (!h) return fail(PANNS_EINVAL, "panns_search_host: NULL handle");
+    const double t0 = now_ms();
+    int rc = check_params(h, p);
+    if (rc) return rc;
+    if (nq == 0) {
+        if (stats) memset(stats, 0, sizeof(*stats));
+        return PANNS_OK;
+    }
+    if (!queries || !out_ids) return fail(PANNS_EINVAL, "panns_search_host: NULL argument");
+    CU(cudaSetDevice(h->device));
+    std::vector<uint32_t> buf;
+    const uint32_t *ids = nullptr;
+    uint32_t count = 0, stride = 0;
+    rc = resolve_init(h, p, init_ids, nq, buf, ids, count, stride);
+    if (rc) return rc;
+    DevBuf<float> q;
+    rc = upload_chain_major(h, queries, nq, h->d, q);
+    if (rc) return rc;
+    CU(h->out.ensure((size_t) nq * p->K));
+    CU(h->stats.ensure(nq));
+    rc = launch_search(h, p, q.p, nq, ids, count, stride, h->out.p, h->stats.p, h->stream, true);
+    if (rc) return rc;
+    rc = finish(h, nq, p->K, out_ids, stats, t0);
+    h->raw.release();
+    return rc;
+}
+
+int panns_search_device(panns_index *h, const panns_search_params *p, const float *d_queries,
+                        uint32_t nq, const uint32_t *init_ids, uint32_t *d_out_ids, void *stream,
+                        panns_stats *stats) {
+    (void) h; (void) p; (void) d_queries; (void) nq; (void) init_ids; (void) d_out_ids; (void) stream;
+    (void) stats;
+    return fail(PANNS_EINVAL, "panns_search_device: not available in this build");
+}
+
+int panns_recall(const uint32_t *result_ids, uint32_t nq, uint32_t K, const uint32_t *true_ids,
+                 uint32_t true_k, uint32_t L, uint32_t at, double *out) {
+    if (!result_ids || !true_ids || !out) return fail(PANNS_EINVAL, "panns_recall: NULL argument");
+    if (at == 0 || at > true_k || at > 100) return fail(PANNS_EINVAL, "panns_recall: bad k");
+    if (nq == 0) {
+        *out = 0.0;
+        return PANNS_OK;
+    }
+    const uint32_t prefix = std::min(std::min(L, 100u), std::min(K, at));
+    double hits = 0;
+    for (uint32_t q = 0; q < nq; ++q) {
+        const uint32_t *t = true_ids + (size_t) q * true_k;
+        const uint32_t *r = result_ids + (size_t) q * K;
+        for (uint32_t i = 0; i < at; ++i)
+            for (uint32_t j = 0; j < prefix; ++j)
+                if (r[j] == t[i]) {
+                    hits += 1;
+                    break;
+                }
+    }
+    *out = hits / ((double) at * nq);
+    return PANNS_OK;
+}
+
+int panns_load_true_nn(const char *path, uint32_t *nq, uint32_t *K, uint32_t *ids, float *dists) {
+    if (!path || !nq || !K) return fail(PANNS_EINVAL, "panns_load_true_nn: NULL argument");
+    FILE *f = fopen(path, "rb");
+    if (!f) return fail(PANNS_EIO, std::string("cannot open ") + path);
+    uint32_t hdr[2];
+    if (fread(hdr, 4, 2, f) != 2) {
+        fclose(f);
+        return fail(PANNS_EIO, "truncated true-NN header");
+    }
+    *nq = hdr[0];
+    *K = hdr[1];
+    if (!ids) {
+        fclose(f);
+        return PANNS_OK;
+    }
+    std::vector<uint32_t> rec(2ull * hdr[1]);
+    for (uint32_t q = 0; q < hdr[0]; ++q) {
+        if (fread(rec.data(), 4, rec.size(), f) != rec.size()) {
+            fclose(f);
+            return fail(PANNS_EIO, "truncated true-NN body");
+        }
+        for (uint32_t i = 0; i < hdr[1]; ++i) {
+            ids[(size_t) q * hdr[1] + i] = rec[2 * i];
+            if (dists) memcpy(dists + (size_t) q * hdr[1] + i, &rec[2 * i + 1], 4);
+        }
+    }
+    fclose(f);
+    return PANNS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,546 @@
+// Persistent best-first search over an NSG graph, one warp per query.
+//
+// Semantics (exact, ID-identical to the reference's deterministic forms):
+//   * PANNS top-M at one thread (M = 1: sequential search, PSS_v5 at T = 1):
+//     core/Searching.202011241533.top_m_pure.cpp:1881-1965,
+//     core/Searching.202102022027.PSS_v5.dist_thresh.profiling.cpp:1218-1515.
+//     Queue order (dist, id) (include/Candidate.h:11-28); a neighbour is
+//     rejected when dist > the L-th distance; k = nk <= last_k ? nk : last_k + 1.
+//   * efanna2e IndexNSG::Search / SearchWithOptGraph
+//     (include/efanna2e/index_nsg.cpp:452-611): order by distance only, a new
+//     element after existing equal distances (InsertIntoPool,
+//     include/efanna2e/neighbor.h:103-131), rejected when dist >= the L-th.
+//
+// Why a step can be done in parallel: inside one step the reference inserts
+// the freshly computed neighbours one by one into a full, sorted queue of L,
+// each against the live L-th element. That sequence always leaves the queue
+// equal to the L best of (old queue + all fresh neighbours), and the lowest
+// insert position it reports equals the final position of the best fresh
+// element when that element survives (and L otherwise). So the warp computes
+// all fresh distances of the step at once, sorts the survivors and merges
+// them in one rank-based pass; chunked merges give the same result.
+//
+// HBM layout (built by layout kernels in panns_abi.cu):
+//   vec   n x (CL*8) float4, "chain-major": float4 number 8*i + c of a row holds
+//         terms 4i..4i+3 of lane accumulator c of the reference's 8-lane
+//         distance loop, so the 8 threads of a vertex read one 128-byte line
+//         per load and each thread runs its lane's FMA chain in the reference
+//         order. Padding terms are zero (an FMA with 0*0 leaves a lane as is).
+//   norm  n float32, ||v||^2 in the same lane order (norm-trick distance).
+//   head  n x 16 u32: degree, then the first 15 neighbour ids (one 64-byte
+//         read per expansion); ovf_off/ovf: the rest of longer rows (CSR).
+//
+// Per warp (shared memory): the queue (L x (dist f32, id u32 with bit 31 =
+// checked)), a buffer of fresh candidates, staged head rows. Per warp slot in
+// global memory: a visited bitset of n bits plus the list of its words that
+// went from zero to non-zero, so only those are cleared after the query.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace panns {
+
+constexpr uint32_t kChecked = 0x80000000u;
+constexpr uint32_t kIdMask = 0x7fffffffu;
+constexpr uint32_t kFull = 0xffffffffu;
+constexpr int kHeadWords = 16;   // degree + 15 neighbours
+constexpr int kHeadNbrs = kHeadWords - 1;
+constexpr int kBuf = 256;        // fresh-candidate buffer per warp
+constexpr int kCandGroup = 16;   // candidates whose head rows are staged at once
+constexpr int kMaxM = 64;
+
+enum { ORDER_PANNS = 0, ORDER_EFANNA = 1 };
+enum { KIND_IP = 0, KIND_L2 = 1 };
+
+// Error bits written to SearchArgs::error.
+enum : uint32_t { ERR_BAD_ID = 1u, ERR_BAD_INIT = 2u };
+
+struct SearchArgs {
+    const float4 *vec;        // n x (CL*8) float4
+    const float *norms;       // n (KIND_IP)
+    const uint32_t *head;     // n x 16
+    const uint64_t *ovf_off;  // n
+    const uint32_t *ovf;      // overflow neighbours
+    uint32_t n;
+    const float4 *queries;    // nq x (CL*8) float4, chain-major
+    uint32_t nq;
+    const uint32_t *init_ids; // L ids, or nq x L when init_stride == L
+    uint32_t init_stride;
+    uint32_t K, L, M;
+    uint32_t *out_ids;        // nq x K
+    uint4 *out_stats;         // nq x {n_dist, n_expand, n_edges, n_iter}
+    uint32_t *visited;        // slots x vis_words
+    uint32_t vis_words;
+    uint32_t *dirty;          // slots x dirty_cap
+    uint32_t dirty_cap;
+    uint32_t *counter;        // work-stealing query counter
+    uint32_t *error;          // ERR_* bits
+    uint32_t queue_cap;       // shared-memory queue entries per warp (>= L)
+};
+
+// Bytes of shared memory one warp needs.
+__host__ __device__ inline uint32_t warp_smem_bytes(uint32_t queue_cap) {
+    return queue_cap * 8u                 // queue dist + id
+           + kBuf * 12u                   // buffer dist + id + key
+           + kCandGroup * kHeadWords * 4u // staged head rows
+           + kMaxM * 4u                   // picked candidate ids
+           + 64u * 4u;                    // prefix sums / scratch
+}
+
+struct WarpMem {
+    float *qd;
+    uint32_t *qi;
+    float *bd;
+    uint32_t *bi;
+    uint32_t *bk;
+    uint32_t *hrow;
+    uint32_t *cand;
+    uint32_t *pre;
+};
+
+__device__ __forceinline__ WarpMem carve(uint8_t *base, uint32_t queue_cap) {
+    WarpMem m;
+    m.qd = reinterpret_cast<float *>(base);
+    m.qi = reinterpret_cast<uint32_t *>(m.qd + queue_cap);
+    m.bd = reinterpret_cast<float *>(m.qi + queue_cap);
+    m.bi = reinterpret_cast<uint32_t *>(m.bd + kBuf);
+    m.bk = m.bi + kBuf;
+    m.hrow = m.bk + kBuf;
+    m.cand = m.hrow + kCandGroup * kHeadWords;
+    m.pre = m.cand + kMaxM;
+    return m;
+}
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// ---------------------------------------------------------------------------
+// Distance of one vertex, computed by the 8 lanes of a group (c = lane & 7 is
+// the lane accumulator this thread owns). Every lane of the group returns it.
+// Lane sum: ((u0 + u1) + u2) + ... + u7; norm trick: -2 * dot + norm, which
+// is one rounding either way because -2 * dot is exact.
+// ---------------------------------------------------------------------------
+template <int KIND, int CL>
+__device__ __forceinline__ float group_distance(const float4 *__restrict__ vec,
+                                                const float *__restrict__ norms, uint32_t v,
+                                                bool active, const float4 (&qv)[CL], int lane) {
+    const int c = lane & 7;
+    float acc = 0.0f;
+    float nrm = 0.0f;
+    if (active) {
+        const float4 *row = vec + (size_t) v * (CL * 8);
+        float4 x[CL];
+#pragma unroll
+        for (int i = 0; i < CL; ++i) x[i] = __ldg(row + 8 * i + c);
+        if (KIND == KIND_IP) nrm = __ldg(norms + v);
+#pragma unroll
+        for (int i = 0; i < CL; ++i) {
+            if (KIND == KIND_IP) {
+                acc = __fmaf_rn(x[i].x, qv[i].x, acc);
+                acc = __fmaf_rn(x[i].y, qv[i].y, acc);
+                acc = __fmaf_rn(x[i].z, qv[i].z, acc);
+                acc = __fmaf_rn(x[i].w, qv[i].w, acc);
+            } else {
+                float t;
+                t = __fsub_rn(x[i].x, qv[i].x); acc = __fmaf_rn(t, t, acc);
+                t = __fsub_rn(x[i].y, qv[i].y); acc = __fmaf_rn(t, t, acc);
+                t = __fsub_rn(x[i].z, qv[i].z); acc = __fmaf_rn(t, t, acc);
+                t = __fsub_rn(x[i].w, qv[i].w); acc = __fmaf_rn(t, t, acc);
+            }
+        }
+    }
+    const int base = lane & ~7;
+    float s = __shfl_sync(kFull, acc, base);
+#pragma unroll
+    for (int j = 1; j < 8; ++j) s = __fadd_rn(s, __shfl_sync(kFull, acc, base + j));
+    if (KIND == KIND_IP) s = __fmaf_rn(-2.0f, s, nrm);
+    return s;
+}
+
+__device__ __forceinline__ bool key_less(float ad, uint32_t ak, float bd, uint32_t bk) {
+    return ad < bd || (ad == bd && ak < bk);
+}
+
+// Number of queue elements that precede a fresh element (d, id).
+template <int ORDER>
+__device__ __forceinline__ uint32_t queue_rank(const float *qd, const uint32_t *qi, uint32_t sz,
+                                               float d, uint32_t id) {
+    uint32_t lo = 0, hi = sz;
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        bool before;
+        if (ORDER == ORDER_PANNS) {
+            float md = qd[mid];
+            before = md < d || (md == d && (qi[mid] & kIdMask) < id);
+        } else {
+            before = qd[mid] <= d;  // older elements stay ahead of equal distances
+        }
+        if (before) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+// Number of sorted fresh elements that precede a queue element (d, id).
+template <int ORDER>
+__device__ __forceinline__ uint32_t fresh_rank(const float *bd, const uint32_t *bi, uint32_t cnt,
+                                               float d, uint32_t id) {
+    uint32_t lo = 0, hi = cnt;
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        bool before;
+        if (ORDER == ORDER_PANNS) {
+            float md = bd[mid];
+            before = md < d || (md == d && bi[mid] < id);
+        } else {
+            before = bd[mid] < d;
+        }
+        if (before) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+// Bitonic sort of (bd, bk)[0..cnt) by (dist, key), carrying bi along when
+// carry_ids; the padding up to the next power of two holds (+inf, ~0).
+__device__ void warp_sort(float *bd, uint32_t *bi, uint32_t *bk, uint32_t cnt, bool carry_ids,
+                          int lane) {
+    if (cnt <= 1) return;
+    uint32_t n = 1;
+    while (n < cnt) n <<= 1;
+    for (uint32_t i = cnt + lane; i < n; i += 32) {
+        bd[i] = __int_as_float(0x7f800000);
+        bi[i] = kFull;
+        bk[i] = kFull;
+    }
+    __syncwarp();
+    for (uint32_t k = 2; k <= n; k <<= 1) {
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t i = lane; i < n; i += 32) {
+                uint32_t ixj = i ^ j;
+                if (ixj > i) {
+                    float ad = bd[i], xd = bd[ixj];
+                    uint32_t ak = bk[i], xk = bk[ixj];
+                    bool up = (i & k) == 0;
+                    bool sw = up ? key_less(xd, xk, ad, ak) : key_less(ad, ak, xd, xk);
+                    if (sw) {
+                        bd[i] = xd; bd[ixj] = ad;
+                        bk[i] = xk; bk[ixj] = ak;
+                        if (carry_ids) { uint32_t t = bi[i]; bi[i] = bi[ixj]; bi[ixj] = t; }
+                    }
+                }
+            }
+            __syncwarp();
+        }
+    }
+}
+
+// Merge the sorted fresh elements (bd, bi)[0..cnt) into the queue of size *sz
+// (capacity L). Returns the position of the first fresh element if it was
+// inserted (< L), else L. Uses bk as scratch.
+template <int ORDER>
+__device__ uint32_t warp_merge(const WarpMem &m, uint32_t *sz, uint32_t L, uint32_t cnt, int lane) {
+    const uint32_t qsz = *sz;
+    if (cnt == 0) return L;
+    // Merged position of each fresh element: its index plus its rank in the old queue.
+    for (uint32_t i = lane; i < cnt; i += 32)
+        m.bk[i] = i + queue_rank<ORDER>(m.qd, m.qi, qsz, m.bd[i], m.bi[i]);
+    __syncwarp();
+    const uint32_t p0 = m.bk[0];
+    if (p0 >= L) return L;
+    // Move queue elements [p0, qsz) to their merged positions, top chunk first;
+    // a chunk is read completely before any of it is written.
+    for (int32_t top = (int32_t) qsz - 1; top >= (int32_t) p0; top -= 32) {
+        const int32_t j = top - lane;
+        float d = 0.f;
+        uint32_t id = 0, np = L;
+        if (j >= (int32_t) p0) {
+            d = m.qd[j];
+            id = m.qi[j];
+            np = (uint32_t) j + fresh_rank<ORDER>(m.bd, m.bi, cnt, d, id & kIdMask);
+        }
+        __syncwarp();
+        if (np < L) {
+            m.qd[np] = d;
+            m.qi[np] = id;
+        }
+        __syncwarp();
+    }
+    for (uint32_t i = lane; i < cnt; i += 32) {
+        const uint32_t np = m.bk[i];
+        if (np < L) {
+            m.qd[np] = m.bd[i];
+            m.qi[np] = m.bi[i];
+        }
+    }
+    __syncwarp();
+    *sz = min(L, qsz + cnt);
+    return p0;
+}
+
+// Visited test-and-set on the slot's bitset; records words that went from 0.
+// Returns true for a vertex not seen before in this query.
+__device__ __forceinline__ bool visit(uint32_t *vis, uint32_t *dirty, uint32_t dirty_cap,
+                                      uint32_t &dcount, uint32_t id, bool valid, int lane) {
+    bool fresh = false, first = false;
+    uint32_t w = 0;
+    if (valid) {
+        w = id >> 5;
+        const uint32_t bit = 1u << (id & 31);
+        const uint32_t old = atomicOr(vis + w, bit);
+        fresh = (old & bit) == 0;
+        first = old == 0;
+    }
+    const uint32_t bm = __ballot_sync(kFull, first);
+    if (first) {
+        const uint32_t pos = dcount + __popc(bm & lanemask_lt());
+        if (pos < dirty_cap) dirty[pos] = w;
+    }
+    dcount += __popc(bm);
+    return fresh;
+}
+
+// Compute distances of the buffered fresh vertices bi[0..nb), keep the ones
+// that can still enter the queue, sort them and merge them. Returns the merge
+// position of the best survivor or L.
+template <int KIND, int ORDER, int CL>
+__device__ uint32_t flush(const SearchArgs &a, const WarpMem &m, uint32_t nb, uint32_t *sz,
+                          bool filter, const float4 (&qv)[CL], int lane) {
+    const int g = lane >> 3;
+    // Distances, 4 vertices per pass (8 lanes each).
+    for (uint32_t b0 = 0; b0 < nb; b0 += 4) {
+        const uint32_t b = b0 + g;
+        const bool act = b < nb;
+        const uint32_t v = act ? m.bi[b] : 0u;
+        const float dist = group_distance<KIND, CL>(a.vec, a.norms, v, act, qv, lane);
+        if (act && (lane & 7) == 0) m.bd[b] = dist;
+    }
+    __syncwarp();
+    // Keep the survivors, in arrival order.
+    const uint32_t L = a.L;
+    const float bound = (filter && *sz >= L) ? m.qd[L - 1] : __int_as_float(0x7f800000);
+    uint32_t cnt = 0;
+    for (uint32_t b0 = 0; b0 < nb; b0 += 32) {
+        const uint32_t b = b0 + lane;
+        float d = 0.f;
+        uint32_t id = 0;
+        bool keep = false;
+        if (b < nb) {
+            d = m.bd[b];
+            id = m.bi[b];
+            keep = !filter || *sz < L || (ORDER == ORDER_PANNS ? !(d > bound) : d < bound);
+        }
+        const uint32_t bm = __ballot_sync(kFull, keep);
+        __syncwarp();
+        if (keep) {
+            const uint32_t pos = cnt + __popc(bm & lanemask_lt());
+            m.bd[pos] = d;
+            m.bi[pos] = id;
+            m.bk[pos] = ORDER == ORDER_PANNS ? id : pos;
+        }
+        cnt += __popc(bm);
+        __syncwarp();
+    }
+    if (cnt == 0) return L;
+    warp_sort(m.bd, m.bi, m.bk, cnt, true, lane);
+    return warp_merge<ORDER>(m, sz, L, cnt, lane);
+}
+
+// One query, run by one warp.
+template <int KIND, int ORDER, int CL>
+__device__ void search_one(const SearchArgs &a, const WarpMem &m, uint32_t q, uint32_t *vis,
+                           uint32_t *dirty, int lane) {
+    const uint32_t L = a.L;
+    float4 qv[CL];
+    {
+        const float4 *qrow = a.queries + (size_t) q * (CL * 8);
+#pragma unroll
+        for (int i = 0; i < CL; ++i) qv[i] = __ldg(qrow + 8 * i + (lane & 7));
+    }
+    uint32_t dcount = 0;
+    uint32_t n_dist = 0, n_expand = 0, n_edges = 0, n_iter = 0;
+    uint32_t sz = 0;
+
+    // Initial queue: the L init ids, all marked visited, sorted (init order
+    // breaks equal distances for efanna2e).
+    const uint32_t *init = a.init_ids + (size_t) q * a.init_stride;
+    uint32_t nb = 0;
+    for (uint32_t i0 = 0; i0 < L; i0 += 32) {
+        const uint32_t i = i0 + lane;
+        const bool valid = i < L;
+        uint32_t id = valid ? __ldg(init + i) : 0u;
+        bool ok = valid && id < a.n;
+        if (valid && !ok) atomicOr(a.error, ERR_BAD_INIT);
+        visit(vis, dirty, a.dirty_cap, dcount, id, ok, lane);
+        const uint32_t bm = __ballot_sync(kFull, ok);
+        if (ok) m.bi[nb + __popc(bm & lanemask_lt())] = id;
+        nb += __popc(bm);
+        __syncwarp();
+        if (nb > kBuf - 32 || i0 + 32 >= L) {
+            n_dist += nb;
+            flush<KIND, ORDER, CL>(a, m, nb, &sz, false, qv, lane);
+            nb = 0;
+        }
+    }
+
+    uint32_t k = 0;
+    const uint32_t M = a.M;
+    for (;;) {
+        // Pick up to M unchecked candidates at positions >= k.
+        uint32_t cnt = 0, last_k = L;
+        for (uint32_t p0 = k; p0 < sz && cnt < M; p0 += 32) {
+            const uint32_t p = p0 + lane;
+            const bool un = p < sz && !(m.qi[p] & kChecked);
+            const uint32_t bm = __ballot_sync(kFull, un);
+            const uint32_t take = min((uint32_t) __popc(bm), M - cnt);
+            const uint32_t r = __popc(bm & lanemask_lt());
+            if (un && r < take) {
+                const uint32_t id = m.qi[p];
+                m.qi[p] = id | kChecked;
+                m.cand[cnt + r] = id;
+                if (r == take - 1) m.pre[63] = p;
+            }
+            __syncwarp();
+            if (take) last_k = m.pre[63];
+            cnt += take;
+            __syncwarp();
+        }
+        if (cnt == 0) break;
+        ++n_iter;
+        n_expand += cnt;
+        uint32_t nk = L;
+        nb = 0;
+        for (uint32_t c0 = 0; c0 < cnt; c0 += kCandGroup) {
+            const uint32_t gc = min((uint32_t) kCandGroup, cnt - c0);
+            // Stage the head rows: 2 candidates per warp-wide load, all loads
+            // issued before the first store.
+            {
+                uint32_t hv[kCandGroup / 2];
+#pragma unroll
+                for (int r = 0; r < kCandGroup / 2; ++r) {
+                    const uint32_t j = 2 * r + (lane >> 4);
+                    hv[r] = j < gc ? __ldg(a.head + (size_t) m.cand[c0 + j] * kHeadWords + (lane & 15))
+                                   : 0u;
+                }
+#pragma unroll
+                for (int r = 0; r < kCandGroup / 2; ++r) {
+                    const uint32_t j = 2 * r + (lane >> 4);
+                    if (j < gc) m.hrow[j * kHeadWords + (lane & 15)] = hv[r];
+                }
+            }
+            __syncwarp();
+            // Prefix sums of the head-row neighbour counts.
+            uint32_t deg = 0, hcount = 0;
+            if (lane < (int) gc) {
+                deg = m.hrow[lane * kHeadWords];
+                hcount = min(deg, (uint32_t) kHeadNbrs);
+            }
+            uint32_t incl = hcount;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t t = __shfl_up_sync(kFull, incl, o);
+                if (lane >= o) incl += t;
+            }
+            const uint32_t total = __shfl_sync(kFull, incl, 31);
+            if (lane < (int) gc) m.pre[lane] = incl - hcount;
+            uint32_t degsum = deg;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) degsum += __shfl_xor_sync(kFull, degsum, o);
+            n_edges += gc + degsum;
+            __syncwarp();
+            // Head-row neighbours, in (candidate, slot) order.
+            for (uint32_t f0 = 0; f0 < total; f0 += 32) {
+                const uint32_t f = f0 + lane;
+                bool valid = f < total;
+                uint32_t id = 0;
+                if (valid) {
+                    uint32_t j = 0;
+                    while (j + 1 < gc && m.pre[j + 1] <= f) ++j;
+                    id = m.hrow[j * kHeadWords + 1 + (f - m.pre[j])];
+                    if (id >= a.n) {
+                        atomicOr(a.error, ERR_BAD_ID);
+                        valid = false;
+                    }
+                }
+                const bool fresh = visit(vis, dirty, a.dirty_cap, dcount, id, valid, lane);
+                if (nb + 32 > kBuf) {
+                    n_dist += nb;
+                    const uint32_t r = flush<KIND, ORDER, CL>(a, m, nb, &sz, true, qv, lane);
+                    nk = min(nk, r);
+                    nb = 0;
+                }
+                const uint32_t bm = __ballot_sync(kFull, fresh);
+                if (fresh) m.bi[nb + __popc(bm & lanemask_lt())] = id;
+                nb += __popc(bm);
+                __syncwarp();
+            }
+            // Rows longer than the head: the rest from the overflow list.
+            for (uint32_t j = 0; j < gc; ++j) {
+                const uint32_t dj = m.hrow[j * kHeadWords];
+                if (dj <= (uint32_t) kHeadNbrs) continue;
+                const uint64_t off = __ldg(a.ovf_off + m.cand[c0 + j]);
+                for (uint32_t s0 = kHeadNbrs; s0 < dj; s0 += 32) {
+                    const uint32_t s = s0 + lane;
+                    bool valid = s < dj;
+                    uint32_t id = valid ? __ldg(a.ovf + off + (s - kHeadNbrs)) : 0u;
+                    if (valid && id >= a.n) {
+                        atomicOr(a.error, ERR_BAD_ID);
+                        valid = false;
+                    }
+                    const bool fresh = visit(vis, dirty, a.dirty_cap, dcount, id, valid, lane);
+                    if (nb + 32 > kBuf) {
+                        n_dist += nb;
+                        const uint32_t r = flush<KIND, ORDER, CL>(a, m, nb, &sz, true, qv, lane);
+                        nk = min(nk, r);
+                        nb = 0;
+                    }
+                    const uint32_t bm = __ballot_sync(kFull, fresh);
+                    if (fresh) m.bi[nb + __popc(bm & lanemask_lt())] = id;
+                    nb += __popc(bm);
+                    __syncwarp();
+                }
+            }
+            __syncwarp();
+        }
+        if (nb) {
+            n_dist += nb;
+            const uint32_t r = flush<KIND, ORDER, CL>(a, m, nb, &sz, true, qv, lane);
+            nk = min(nk, r);
+            nb = 0;
+        }
+        k = nk <= last_k ? nk : last_k + 1;
+    }
+
+    // Results and counters.
+    for (uint32_t i = lane; i < a.K; i += 32) a.out_ids[(size_t) q * a.K + i] = m.qi[i] & kIdMask;
+    if (lane == 0 && a.out_stats) a.out_stats[q] = make_uint4(n_dist, n_expand, n_edges, n_iter);
+    // Clear the visited words this query set.
+    if (dcount <= a.dirty_cap) {
+        for (uint32_t i = lane; i < dcount; i += 32) vis[dirty[i]] = 0u;
+    } else {
+        for (uint32_t i = lane; i < a.vis_words; i += 32) vis[i] = 0u;
+    }
+    __syncwarp();
+}
+
+template <int KIND, int ORDER, int CL>
+__global__ void __launch_bounds__(256) search_kernel(SearchArgs a) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    const int lane = threadIdx.x & 31;
+    const int wid = threadIdx.x >> 5;
+    const WarpMem m = carve(smem + (size_t) wid * warp_smem_bytes(a.queue_cap), a.queue_cap);
+    const uint32_t slot = blockIdx.x * (blockDim.x >> 5) + wid;
+    uint32_t *vis = a.visited + (size_t) slot * a.vis_words;
+    uint32_t *dirty = a.dirty + (size_t) slot * a.dirty_cap;
+    for (;;) {
+        uint32_t q = 0;
+        if (lane == 0) q = atomicAdd(a.counter, 1u);
+        q = __shfl_sync(kFull, q, 0);
+        if (q >= a.nq) break;
+        search_one<KIND, ORDER, CL>(a, m, q, vis, dirty, lane);
+    }
+}
+
+}  // namespace panns

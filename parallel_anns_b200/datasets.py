@@ -140,8 +140,9 @@ def mrng_prune(base: np.ndarray, knn_ids: np.ndarray, knn_d: np.ndarray, R: int,
             kept += ok.long()
         keep_np = keep.cpu().numpy()
         ids_np = knn_ids[s:s + block]
-        for r in range(ids_np.shape[0]):
-            lists.append(ids_np[r][keep_np[r]].astype(np.uint32))
+        cnt = keep_np.sum(1)
+        flat = ids_np[keep_np].astype(np.uint32)  # row-major: each row's kept ids in order
+        lists.extend(np.split(flat, np.cumsum(cnt)[:-1]))
     return lists
 
 
@@ -151,24 +152,27 @@ def medoid(base: np.ndarray) -> int:
     return int(np.argmin(d))
 
 
+def _reached_from(lists: list, src: int, n: int) -> np.ndarray:
+    from scipy.sparse import csr_matrix
+    from scipy.sparse.csgraph import breadth_first_order
+    deg = np.array([len(l) for l in lists], dtype=np.int64)
+    indptr = np.zeros(n + 1, dtype=np.int64)
+    np.cumsum(deg, out=indptr[1:])
+    idx = np.concatenate(lists).astype(np.int64) if indptr[-1] else np.zeros(0, np.int64)
+    m = csr_matrix((np.ones(idx.shape[0], dtype=np.int8), idx, indptr), shape=(n, n))
+    order = breadth_first_order(m, src, directed=True, return_predecessors=False)
+    reached = np.zeros(n, dtype=bool)
+    reached[order] = True
+    return reached
+
+
 def repair_reachability(lists: list, entry: int, knn_ids: np.ndarray) -> int:
     """Give every vertex unreachable from ``entry`` an in-edge; returns edges added."""
     n = len(lists)
-    reached = np.zeros(n, dtype=bool)
-
-    def sweep(src: int):
-        dq = deque([src])
-        reached[src] = True
-        while dq:
-            u = dq.popleft()
-            for w in lists[u]:
-                if not reached[w]:
-                    reached[w] = True
-                    dq.append(int(w))
-
-    sweep(entry)
+    reached = _reached_from(lists, entry, n)
     added = 0
-    for u in range(n):
+    for u in np.nonzero(~reached)[0]:
+        u = int(u)
         if reached[u]:
             continue
         parent = entry
@@ -178,7 +182,15 @@ def repair_reachability(lists: list, entry: int, knn_ids: np.ndarray) -> int:
                 break
         lists[parent] = np.append(lists[parent], np.uint32(u))
         added += 1
-        sweep(u)
+        # mark everything u reaches (only not-yet-reached vertices are walked)
+        dq = deque([u])
+        reached[u] = True
+        while dq:
+            x = dq.popleft()
+            for w in lists[x]:
+                if not reached[w]:
+                    reached[w] = True
+                    dq.append(int(w))
     return added
 
 

@@ -1,0 +1,112 @@
+"""The CPU oracle is pinned to the reference: it must reproduce, bit for bit,
+the reference's distances and norms and, id for id, the result lists and
+distance counts the reference produced for the committed golden fixtures
+(tests/golden/, generated by tests/golden/make_golden.py from the reference
+sources). Where the reference checker binaries are present (oracle/_ref), they
+are re-run and must reproduce the fixtures too."""
+import ctypes
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import GOLDEN, golden_ids, load_case
+
+CASES = ["mix3k_d96", "mix1k_d24", "u8_1k_d128"]
+
+
+def _oracle_run(form, spec, base, q, G):
+    a = spec["args"]
+    b = spec["binary"]
+    K, L = a["K"], a["L"]
+    if b in ("ref_pss", "ref_pss_lg"):
+        kind = O.DIST_IP_NORM if b == "ref_pss" else O.DIST_L2
+        return O.search_pss(base, G, q, K, L, a.get("L_local", L), a["X"], a["T"], kind=kind)
+    if b == "ref_topm":
+        M = a.get("M", 1) if a["mode"] != "simple" else 1
+        return O.search_top_m(base, G, q, K, L, M)
+    kind = O.DIST_L2 if a["mode"] == "search" else O.DIST_IP_NORM
+    return O.search_efanna(base, G, q, K, L, kind=kind)
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_distance_bits_match_reference(case):
+    base, q, g, _ = load_case(case)
+    d = os.path.join(GOLDEN, case)
+    ids = np.fromfile(os.path.join(d, "dist_ids.u32"), dtype=np.uint32)
+    ref_norm = np.fromfile(os.path.join(d, "norms.f32"), dtype=np.float32)
+    nrm = O.norms(base)
+    assert np.array_equal(nrm[ids].view(np.uint32), ref_norm.view(np.uint32))
+    for fname, kind in (("dist_ip.f32", O.DIST_IP_NORM), ("dist_l2.f32", O.DIST_L2)):
+        ref = np.fromfile(os.path.join(d, fname), dtype=np.float32).reshape(-1, ids.size)
+        got = np.array([[O.distance(base[i], q[j], nrm[i], kind) for i in ids]
+                        for j in range(ref.shape[0])], dtype=np.float32)
+        assert np.array_equal(got.view(np.uint32), ref.view(np.uint32)), fname
+
+
+def test_unfused_lane_steps_do_not_match():
+    """The pin is meaningful: separate multiply and add give other bits."""
+    base, q, g, _ = load_case("mix3k_d96")
+    d = os.path.join(GOLDEN, "mix3k_d96")
+    ids = np.fromfile(os.path.join(d, "dist_ids.u32"), dtype=np.uint32)
+    ref = np.fromfile(os.path.join(d, "dist_l2.f32"), dtype=np.float32).reshape(-1, ids.size)
+    got = np.array([[O.distance(base[i], q[j], 0.0, O.DIST_L2, fused=0) for i in ids]
+                    for j in range(ref.shape[0])], dtype=np.float32)
+    assert (got != ref).sum() > 0
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_oracle_reproduces_reference_ids(case, golden_manifest):
+    base, q, g, _ = load_case(case)
+    G = O.Graph.from_nsg(g)
+    for form, spec in golden_manifest[case]["forms"].items():
+        got, nd = _oracle_run(form, spec, base, q, G)
+        ref = golden_ids(case, form, spec["args"]["K"])
+        assert np.array_equal(got, ref), f"{case}/{form}: {(got != ref).any(1).sum()} rows differ"
+        assert nd == spec["n_dist"], f"{case}/{form}: n_dist {nd} != {spec['n_dist']}"
+
+
+@pytest.mark.skipif(not O.have_ref(), reason="reference checker binaries not built here")
+@pytest.mark.parametrize("case", ["mix3k_d96", "mix1k_d24"])
+def test_reference_binaries_reproduce_fixtures(case, golden_manifest):
+    d = os.path.join(GOLDEN, case)
+    files = dict(data=os.path.join(d, "base.fvecs"), queries=os.path.join(d, "query.fvecs"),
+                 nsg=os.path.join(d, "graph.nsg"))
+    with tempfile.TemporaryDirectory() as tmp:
+        for form, spec in golden_manifest[case]["forms"].items():
+            ids, st = O.run_ref(spec["binary"], os.path.join(tmp, "o.ids"), **files, **spec["args"])
+            assert np.array_equal(ids, golden_ids(case, form, spec["args"]["K"])), form
+            assert st["n_dist"] == spec["n_dist"], form
+
+
+def test_rand_replay_matches_libc():
+    libc = ctypes.CDLL("libc.so.6")
+    libc.srand(1)
+    r = O.Rand(1)
+    assert all(libc.rand() == r() for _ in range(20000))
+    libc.srand(12345)
+    r = O.Rand(12345)
+    assert all(libc.rand() == r() for _ in range(2000))
+
+
+def test_prepare_init_ids_rules():
+    # entry 2 with neighbours [5, 5, 1] and N = 8: dedup, then 3, 4, ... wrapping
+    from parallel_anns_b200.formats import NSGGraph
+    g = NSGGraph.from_lists(3, 2, [[1], [2], [5, 5, 1], [], [], [0], [], []])
+    G = O.Graph.from_nsg(g)
+    assert O.prepare_init_ids(G, 6).tolist() == [5, 1, 3, 4, 6, 7]
+    assert O.prepare_init_ids(G, 8).tolist() == [5, 1, 3, 4, 6, 7, 0, 2]
+
+
+def test_pss_many_workers_recall_close_to_single(golden_manifest):
+    """PSS_v5 with several queues (deterministic round-robin schedule) stays
+    within a hair of the one-queue recall, as the reference does at T > 1."""
+    base, q, g, tid = load_case("mix3k_d96")
+    G = O.Graph.from_nsg(g)
+    r1, _ = O.search_pss(base, G, q, 100, 200, 200, 1, 1)
+    base_rec = O.recall_at(r1, tid, 200)
+    for T, X in ((2, 1), (4, 2), (8, 4)):
+        rt, _ = O.search_pss(base, G, q, 100, 200, 200, X, T)
+        assert abs(O.recall_at(rt, tid, 200) - base_rec) < 0.01
