@@ -1,0 +1,415 @@
+#!/usr/bin/env python
+"""Benchmark of the batched best-first NSG search on B200.
+
+Workload (batched FP32): N = 1,000,000 base vectors, d = 96, 64-component
+Gaussian mixture (sigma 0.3, unit norm), NSG-style graph R = 50; 10,000
+queries per GPU (weak scaling: rank r searches its own 10,000); K = 100.
+Metric: queries per second at recall@100 >= 0.95 (the smallest L of the
+sweep that reaches it, per M; the fastest (L, M) wins — the reference's
+"lowest runtime with P@100 >= target" rule).
+
+One step = one batched search of all of a rank's queries (one kernel launch).
+``value``: device time of the search kernel (CUDA events) with base, graph
+and queries resident in HBM; the 384 MB base set alone is larger than L2 and
+L2 is also flushed (a 256 MB write) before every step.
+``e2e``: the same search through the C ABI's host-pointer entry point
+(panns_search_host: queries copied host->device, ids copied back), wall time.
+
+``--impl reference`` times the reference's own PSS_v5
+(core/Searching.202102022027.PSS_v5.dist_thresh.profiling.cpp, built from its
+sources into oracle/_ref/ref_pss) on all host cores, on a bounded query sample.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "QPS at recall@100>=0.95, 1M x 96d; learned+BF16 vs plain FP32 GPU vs CPU"
+UNIT = "queries/s"
+RECALL_TARGET = 0.95
+L_SWEEP = [100, 128, 160, 200, 256, 320, 400, 512, 640, 800]
+M_SWEEP = [1, 2, 4, 8, 16]
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def measured_peak_hbm():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.file = None
+
+    def start(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.device)], stdout=self.file, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.file.flush()
+        self.file.seek(0)
+        rows = [r.split(",") for r in self.file.read().strip().splitlines() if r.strip()]
+        os.unlink(self.file.name)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def nproc():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def run_reference_pss(paths, nq, L, T, X=1, reps=1, K=100, timeout=900):
+    """The reference's PSS_v5 binary (oracle/_ref/ref_pss) on the cached files."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_pss")
+    if not os.path.exists(exe):
+        raise FileNotFoundError(exe)
+    env = dict(os.environ, OMP_PROC_BIND="close", OMP_PLACES="cores")
+    with tempfile.TemporaryDirectory() as tmp:
+        args = [exe, f"data={paths['base']}", f"queries={paths['query']}", f"nsg={paths['graph']}",
+                f"truenn={paths['truenn']}", f"K={K}", f"L={L}", f"T={T}", f"X={X}", f"nq={nq}",
+                f"reps={reps}", f"out={os.path.join(tmp, 'ids.bin')}"]
+        r = subprocess.run(args, check=True, capture_output=True, text=True, env=env, timeout=timeout)
+    return json.loads(r.stdout.strip().splitlines()[-1])
+
+
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return "unknown"
+
+
+# ---------------------------------------------------------------------------
+def bench_ours(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from parallel_anns_b200 import native as N
+    from parallel_anns_b200 import workloads
+    from parallel_anns_b200.searching import Index, recall
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=900),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    spec = workloads.spec_batched_fp32_1m(n=args.n, nq=args.nq * world)
+    if rank == 0:
+        W = workloads.build(spec, device=f"cuda:{local}", log=log)
+    barrier()
+    if rank != 0:
+        W = workloads.load(spec)
+    q_all, gt_all = W["queries"], W["gt"]
+    qs = np.ascontiguousarray(q_all[rank * args.nq:(rank + 1) * args.nq])
+    gts = gt_all[rank * args.nq:(rank + 1) * args.nq]
+    nq, d, K = qs.shape[0], qs.shape[1], 100
+
+    ix = Index(local)
+    ix.set_base(W["base"])
+    ix.set_graph(W["graph"])
+    ix.set_queries(qs)
+
+    def run(L, M):
+        mode = N.MODE_NSG_SEQ if M == 1 else N.MODE_TOP_M
+        return ix.search(K=K, L=L, mode=mode, distance=N.DIST_NORM_IP, M=M)
+
+    # Operating point: per M the smallest swept L reaching the recall target;
+    # the fastest of those. Decided on rank 0, shared with every rank.
+    sweep = []
+    if args.L and args.M:
+        choice = (args.L, args.M)
+    else:
+        best = None
+        for M in ([args.M] if args.M else M_SWEEP):
+            for L in ([args.L] if args.L else L_SWEEP):
+                ids, st = run(L, M)
+                ids, st = run(L, M)
+                rec = recall(ids, gts, L, 100)
+                sweep.append({"M": M, "L": L, "recall100": round(rec, 5),
+                              "qps": round(nq / (st["kernel_ms"] / 1e3), 1)})
+                if rec >= RECALL_TARGET:
+                    if best is None or st["kernel_ms"] < best[0]:
+                        best = (st["kernel_ms"], L, M)
+                    break
+        if best is None:
+            best = (0, L_SWEEP[-1], 1)
+        choice = (best[1], best[2])
+    if world > 1:
+        t = torch.tensor(list(choice), dtype=torch.int64, device="cuda")
+        dist.broadcast(t, 0)
+        choice = (int(t[0]), int(t[1]))
+    L, M = choice
+    if rank == 0:
+        log(f"operating point L={L} M={M}; sweep {sweep}")
+
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
+    sampler = ClockSampler(local)
+    for _ in range(args.warmup):
+        run(L, M)
+    sampler.start()
+    barrier()
+    torch.cuda.synchronize()
+    kernel_ms = 0.0
+    tot = {"n_dist": 0, "n_edges": 0, "n_expand": 0, "n_iter": 0}
+    last_ids = None
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        last_ids, st = run(L, M)
+        kernel_ms += st["kernel_ms"]
+        for k in tot:
+            tot[k] += st[k]
+    barrier()
+    torch.cuda.synchronize()
+    kernel_ms_max = max_over_ranks(kernel_ms)
+    rec = recall(last_ids, gts, L, 100)
+
+    # End to end through the host-pointer C ABI call.
+    mode = N.MODE_NSG_SEQ if M == 1 else N.MODE_TOP_M
+    for _ in range(args.warmup):
+        ix.search(qs, K=K, L=L, mode=mode, M=M)
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        ids_e2e, st_e2e = ix.search(qs, K=K, L=L, mode=mode, M=M)
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    clocks = sampler.stop()
+    assert np.array_equal(ids_e2e, last_ids)
+
+    # Roofline of the search kernel: algorithmic bytes per launch
+    # = n_dist * (4d + 4 norm) + 4 * sum(1 + degree) over expansions + nq * (4d + 4K).
+    steps = args.steps
+    alg_bytes = (tot["n_dist"] * (4 * d + 4) + 4 * tot["n_edges"]) / steps + nq * (4 * d + 4 * K)
+    launch_s = kernel_ms / steps / 1e3
+    achieved = alg_bytes / launch_s / 1e9
+    peak, peak_kind = measured_peak_hbm()
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "search_kernel_traffic.json")
+    if os.path.exists(tp):
+        try:
+            with open(tp) as f:
+                tj = json.load(f)
+            if tj.get("L") == L and tj.get("M") == M and tj.get("n") == args.n:
+                traffic = tj["dram_bytes_per_query"] * nq
+        except Exception:
+            traffic = None
+
+    total_q = nq * world * steps
+    value = total_q / (kernel_ms_max / 1e3)
+    e2e_value = total_q / e2e_s
+
+    cpu_base = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu_base = cpu_baseline(W["paths"], L, nq, log)
+
+    if world > 1:
+        dist.barrier()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
+            "steps": steps, "warmup": args.warmup,
+            "ms_per_step": round(kernel_ms_max / steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "batched FP32 search, 1M x 96d mixture64 (sigma 0.3, unit norm), "
+                                   "NSG-style graph R=50, 10k queries per GPU, K=100",
+                       "n": args.n, "d": d, "queries_per_gpu": nq, "K": K, "L": L, "M": M,
+                       "mode": "NSG_SEQ" if M == 1 else "TOP_M", "distance": "NORM_IP",
+                       "recall100": round(rec, 5), "recall_target": RECALL_TARGET,
+                       "avg_degree": round(W["meta"]["avg_degree"], 3), "width": W["meta"]["width"],
+                       "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (384 MB base) and a 256 MB L2 flush before each step",
+                       "sweep": sweep},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": traffic,
+                         "peak_source": peak_kind,
+                         "algorithmic_bytes_per_launch": int(alg_bytes)},
+            "e2e": {"value": round(e2e_value, 1), "unit": UNIT,
+                    "h2d_bytes_per_step": nq * d * 4 + L * 4,
+                    "d2h_bytes_per_step": nq * K * 4 + nq * 16},
+            "gpu_launches": steps,
+            "counts_per_query": {k: round(v / steps / nq, 2) for k, v in tot.items()},
+            "clocks": clocks,
+            "cpu_baseline": cpu_base,
+        }
+        print(json.dumps(line), flush=True)
+    ix.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def cpu_baseline(paths, L, nq_total, log):
+    """The reference's PSS_v5 on every host core, on a bounded query sample
+    (about 10-20 s of CPU work), at the L of the GPU's operating point."""
+    try:
+        T = nproc()
+        probe = run_reference_pss(paths, min(500, nq_total), L, T, X=1)
+        per_q = probe["runtime_s"] / probe["nq"]
+        sample = int(max(200, min(nq_total, 12.0 / max(per_q, 1e-9))))
+        best = None
+        for X in (1, 4):
+            r = run_reference_pss(paths, sample, L, T, X=X)
+            if best is None or r["runtime_s"] < best[1]["runtime_s"]:
+                best = (X, r)
+        X, r = best
+        log(f"cpu baseline: PSS_v5 T={T} X={X} L={L}: {r}")
+        return {"value": round(r["qps"], 1), "unit": UNIT, "cores": T, "kind": "reference",
+                "sample": f"{r['nq']} of the queries, PSS_v5 (L_master=L_local={L}, X={X}, "
+                          f"T={T}), recall@100 {r['recall100']:.4f}, {cpu_model()}"}
+    except Exception as e:  # the baseline is informative; never fail the bench on it
+        log(f"cpu baseline unavailable: {e}")
+        return None
+
+
+# ---------------------------------------------------------------------------
+def bench_reference(args):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    from parallel_anns_b200 import workloads
+    import torch
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_pss")
+    if not os.path.exists(exe):
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "reference checker binaries were not built (oracle/_ref/ref_pss missing)"}))
+        return
+    spec = workloads.spec_batched_fp32_1m(n=args.n, nq=args.nq)
+    dev = f"cuda:{local}" if torch.cuda.is_available() else "cpu"
+    W = workloads.build(spec, device=dev, log=log)
+    T = nproc()
+    # The reference's own operating point: smallest swept L with recall@100 >= 0.95
+    # on a sample, measured by the reference itself.
+    L = args.L
+    if not L:
+        for Lc in L_SWEEP:
+            r = run_reference_pss(W["paths"], min(1000, args.nq), Lc, T)
+            if r["recall100"] >= RECALL_TARGET:
+                L = Lc
+                break
+        L = L or L_SWEEP[-1]
+    probe = run_reference_pss(W["paths"], min(500, args.nq), L, T)
+    per_q = probe["runtime_s"] / probe["nq"]
+    budget_s = 150.0 / max(1, args.steps + args.warmup)
+    sample = int(max(100, min(args.nq, budget_s / max(per_q, 1e-9))))
+    r = run_reference_pss(W["paths"], sample, L, T, X=1, reps=args.warmup + args.steps)
+    times = r["rep_times"][args.warmup:]
+    value = sample * len(times) / sum(times)
+    line = {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(1e3 * sum(times) / len(times), 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": "batched FP32 search, 1M x 96d mixture64 (sigma 0.3, unit norm), "
+                                   "NSG-style graph R=50, 10k queries per GPU, K=100",
+                       "n": args.n, "d": 96, "K": 100, "L": L, "T": T, "X": 1,
+                       "recall100": r["recall100"], "queries_per_step": sample},
+            "cpu_baseline": {"value": round(value, 1), "unit": UNIT, "cores": T, "kind": "reference",
+                             "sample": f"{sample} queries per step, PSS_v5 L_master=L_local={L}, "
+                                       f"X=1, T={T}, {cpu_model()}"},
+            "e2e": {"value": round(value, 1), "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=1_000_000)
+    ap.add_argument("--nq", type=int, default=10_000, help="queries per GPU")
+    ap.add_argument("--L", type=int, default=0, help="fix L (default: recall-driven sweep)")
+    ap.add_argument("--M", type=int, default=0, help="fix M (default: sweep)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        bench_reference(args)
+    else:
+        bench_ours(args)
+
+
+if __name__ == "__main__":
+    main()

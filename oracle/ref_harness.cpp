@@ -29,7 +29,10 @@
 //       every vertex id listed in ids= (a raw u32 file) to out= as f32,
 //       row-major [nq x n_ids]; REF_PSS also writes the vertex norms to
 //       out=.norms.
-// stdout: one JSON line with n_dist, runtime_s, qps, recall100 (if truenn=).
+// stdout: one JSON line with n_dist (of the last repetition), runtime_s (the
+// best repetition), qps, recall100 (if truenn=), rep_times (every repetition,
+// timed like app/PSS_v5_distance_threshold_profiling.cpp:129-152: a
+// std::chrono bracket around prepare_init_ids and the query loop).
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -106,13 +109,17 @@ static double recall100(const char *truenn, const std::vector<std::vector<unsign
     return hit / (100.0 * nq);
 }
 
+static std::vector<double> g_rep_times;
+
 static void report(double secs, unsigned long long n_dist, unsigned nq,
                    const std::vector<std::vector<unsigned>> &res, unsigned L, int threads) {
     double rec = -1.0;
     if (g_args.count("truenn")) rec = recall100(arg_s("truenn"), res, L);
     printf("{\"n_dist\": %llu, \"runtime_s\": %.9f, \"qps\": %.3f, \"recall100\": %.6f, "
-           "\"threads\": %d, \"nq\": %u}\n",
+           "\"threads\": %d, \"nq\": %u, \"rep_times\": [",
            n_dist, secs, nq / secs, rec, threads, nq);
+    for (size_t i = 0; i < g_rep_times.size(); ++i) printf(i ? ", %.9f" : "%.9f", g_rep_times[i]);
+    printf("]}\n");
 }
 
 int main(int argc, char **argv) {
@@ -208,6 +215,7 @@ int main(int argc, char **argv) {
         }
         auto e = std::chrono::high_resolution_clock::now();
         double secs = std::chrono::duration<double>(e - s).count();
+        g_rep_times.push_back(secs);
         if (secs < best) best = secs;
         n_dist = engine.count_distance_computation_;
     }
@@ -239,6 +247,7 @@ int main(int argc, char **argv) {
         }
         auto e = std::chrono::high_resolution_clock::now();
         double secs = std::chrono::duration<double>(e - s).count();
+        g_rep_times.push_back(secs);
         if (secs < best) best = secs;
         n_dist = engine.count_distance_computation_;
     }

@@ -119,6 +119,7 @@ struct panns_index {
     // queries
     uint32_t nq = 0, qd = 0;
     DevBuf<float> queries;  // chain-major
+    DevBuf<float> hq;       // chain-major staging of host-pointer queries
     // scratch
     DevBuf<float> raw;      // staging for permutation
     DevBuf<uint32_t> visited, dirty, counter, error, init, out;
@@ -694,16 +695,13 @@ int panns_search_host(panns_index *h, const panns_search_params *p, const float 
     uint32_t count = 0, stride = 0;
     rc = resolve_init(h, p, init_ids, nq, buf, ids, count, stride);
     if (rc) return rc;
-    DevBuf<float> q;
-    rc = upload_chain_major(h, queries, nq, h->d, q);
+    rc = upload_chain_major(h, queries, nq, h->d, h->hq);
     if (rc) return rc;
     CU(h->out.ensure((size_t) nq * p->K));
     CU(h->stats.ensure(nq));
-    rc = launch_search(h, p, q.p, nq, ids, count, stride, h->out.p, h->stats.p, h->stream, true);
+    rc = launch_search(h, p, h->hq.p, nq, ids, count, stride, h->out.p, h->stats.p, h->stream, true);
     if (rc) return rc;
-    rc = finish(h, nq, p->K, out_ids, stats, t0);
-    h->raw.release();
-    return rc;
+    return finish(h, nq, p->K, out_ids, stats, t0);
 }
 
 int panns_search_device(panns_index *h, const panns_search_params *p, const float *d_queries,

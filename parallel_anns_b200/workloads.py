@@ -1,0 +1,78 @@
+"""Benchmark workloads: seeded synthetic stand-ins for the reference's datasets.
+
+``batched_fp32_1m``: N = 1,000,000 base vectors, d = 96, from a 64-component
+isotropic Gaussian mixture (means ~ N(0, 1), sigma = 0.3), L2-normalised;
+queries from the same mixture; NSG-style graph with R = 50 built by
+``datasets.build_nsg_graph`` (exact 64-NN, MRNG prune, medoid entry,
+reachability repair); ground truth = top-100 by float64 brute force.
+
+Files are written in the reference's formats (fvecs, .nsg, true-NN) to a cache
+directory so that the reference's own binaries can read them and a second
+process on the same host reuses them.
+"""
+from __future__ import annotations
+
+import json
+import os
+import time
+
+import numpy as np
+
+from . import datasets as ds
+from . import formats as fm
+
+CACHE = os.environ.get("PANNS_BENCH_CACHE", "/tmp/panns_b200_bench")
+
+
+def spec_batched_fp32_1m(n=1_000_000, nq=10_000, d=96):
+    return {"name": f"mixture64_n{n}_d{d}_q{nq}_R50", "n": n, "d": d, "nq": nq, "R": 50,
+            "knn_k": 64, "components": 64, "sigma": 0.3, "base_seed": 1001, "query_seed": 2001,
+            "gt_k": 100}
+
+
+def paths(spec):
+    root = os.path.join(CACHE, spec["name"])
+    return {k: os.path.join(root, v) for k, v in
+            dict(root="", base="base.fvecs", query="query.fvecs", graph="graph.nsg",
+                 truenn="truenn.bin", meta="meta.json").items()}
+
+
+def build(spec, device=None, log=print):
+    """Build (or load from the cache) a workload; returns a dict of arrays + paths."""
+    p = paths(spec)
+    if os.path.exists(p["meta"]):
+        with open(p["meta"]) as f:
+            meta = json.load(f)
+        if meta.get("spec") == spec:
+            return load(spec)
+    os.makedirs(p["root"], exist_ok=True)
+    t0 = time.time()
+    base = ds.gaussian_mixture(spec["n"], spec["d"], spec["components"], spec["sigma"],
+                               seed=spec["base_seed"], means_seed=spec["base_seed"])
+    q = ds.gaussian_mixture(spec["nq"], spec["d"], spec["components"], spec["sigma"],
+                            seed=spec["query_seed"], means_seed=spec["base_seed"])
+    t1 = time.time()
+    g = ds.build_nsg_graph(base, R=spec["R"], knn_k=spec["knn_k"], device=device)
+    t2 = time.time()
+    import torch
+    gt_ids, gt_d = ds.exact_knn(base, q, spec["gt_k"], device=device, dtype=torch.float64, block=512)
+    t3 = time.time()
+    fm.write_fvecs(p["base"], base)
+    fm.write_fvecs(p["query"], q)
+    fm.write_nsg(p["graph"], g)
+    fm.write_true_nn(p["truenn"], gt_ids, gt_d.astype(np.float32))
+    meta = {"spec": spec, "width": g.width, "entry": g.entry, "avg_degree": float(g.nbrs.size / g.n),
+            "build_s": {"generate": t1 - t0, "graph": t2 - t1, "ground_truth": t3 - t2}}
+    with open(p["meta"], "w") as f:
+        json.dump(meta, f)
+    log(f"workload {spec['name']}: built in {time.time() - t0:.1f}s {meta['build_s']}")
+    return {"base": base, "queries": q, "graph": g, "gt": gt_ids, "paths": p, "meta": meta}
+
+
+def load(spec):
+    p = paths(spec)
+    with open(p["meta"]) as f:
+        meta = json.load(f)
+    return {"base": fm.read_fvecs(p["base"]), "queries": fm.read_fvecs(p["query"]),
+            "graph": fm.read_nsg(p["graph"]), "gt": fm.read_true_nn(p["truenn"])[0], "paths": p,
+            "meta": meta}
