@@ -43,17 +43,57 @@ __host__ __device__ inline int chain_term_element(int d, int c, int k) {
     return c + 8 * k;
 }
 
+// out row r = chain-major copy of raw row (rowmap ? rowmap[r] : r).
 __global__ void permute_rows_kernel(const float *__restrict__ raw, float *__restrict__ out,
-                                    uint64_t rows, int d, int dpad) {
+                                    uint64_t rows, int d, int dpad,
+                                    const uint32_t *__restrict__ rowmap) {
     const uint64_t total = rows * (uint64_t) dpad;
     for (uint64_t t = blockIdx.x * (uint64_t) blockDim.x + threadIdx.x; t < total;
          t += (uint64_t) gridDim.x * blockDim.x) {
         const uint64_t r = t / dpad;
+        const uint64_t src = rowmap ? rowmap[r] : r;
         const int p = (int) (t % dpad);
         const int chunk = p >> 2, i = chunk >> 3, c = chunk & 7;
         const int k = 4 * i + (p & 3);
         const int e = chain_term_element(d, c, k);
-        out[t] = e >= 0 ? raw[r * d + e] : 0.0f;
+        out[t] = e >= 0 ? raw[src * d + e] : 0.0f;
+    }
+}
+
+// Locality order, step 1: the nearest of C pivot vertices for every vertex
+// (squared L2 on the raw rows; a layout heuristic, not part of the search
+// semantics). One warp per vertex, lanes stride over the pivots.
+__global__ void nearest_pivot_kernel(const float *__restrict__ raw, uint32_t n, int d,
+                                     const uint32_t *__restrict__ pivots, uint32_t C,
+                                     uint32_t *__restrict__ cell) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t warps = (uint64_t) gridDim.x * (blockDim.x >> 5);
+    for (uint64_t v = blockIdx.x * (uint64_t) (blockDim.x >> 5) + (threadIdx.x >> 5); v < n;
+         v += warps) {
+        const float *x = raw + v * d;
+        float best = __int_as_float(0x7f800000);
+        uint32_t arg = 0;
+        for (uint32_t p = lane; p < C; p += 32) {
+            const float *y = raw + (uint64_t) pivots[p] * d;
+            float s = 0.f;
+            for (int j = 0; j < d; ++j) {
+                const float t = x[j] - y[j];
+                s = fmaf(t, t, s);
+            }
+            if (s < best) {
+                best = s;
+                arg = p;
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const float ob = __shfl_xor_sync(0xffffffffu, best, o);
+            const uint32_t oa = __shfl_xor_sync(0xffffffffu, arg, o);
+            if (ob < best || (ob == best && oa < arg)) {
+                best = ob;
+                arg = oa;
+            }
+        }
+        if (lane == 0) cell[v] = arg;
     }
 }
 
@@ -107,9 +147,12 @@ struct panns_index {
     int num_sms = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    // base vectors
+    // base vectors (raw rows stay on the device until the index is finalised)
     uint32_t n = 0, d = 0, dpad = 0, storage = 0;
-    DevBuf<float> vec, norms;
+    DevBuf<float> base_raw, vec, norms;
+    bool ready = false;             // vec/norms/head built for the current base + graph
+    std::vector<uint32_t> perm, inv;  // device id -> original id, and back
+    DevBuf<uint32_t> orig;
     // graph
     uint32_t width = 0, entry = 0, gn = 0;
     std::vector<uint64_t> off;
@@ -177,7 +220,7 @@ static int upload_chain_major(panns_index *h, const float *rows, uint64_t count,
     const uint64_t total = count * dpad;
     const int blocks = (int) std::min<uint64_t>((total + 255) / 256, (uint64_t) h->num_sms * 32);
     permute_rows_kernel<<<std::max(blocks, 1), 256, 0, h->stream>>>(h->raw.p, dst.p, count, (int) d,
-                                                                   (int) dpad);
+                                                                   (int) dpad, nullptr);
     CU(cudaGetLastError());
     return PANNS_OK;
 }
@@ -191,19 +234,19 @@ int panns_set_base(panns_index *h, const float *data, uint32_t n, uint32_t d, ui
     if (storage != PANNS_STORE_FP32)
         return fail(PANNS_EINVAL, "panns_set_base: only FP32 storage is available in this build");
     if (h->qd && h->qd != d) return fail(PANNS_EINVAL, "panns_set_base: dimension differs from the queries");
+    if (h->gn && h->gn != n)
+        return fail(PANNS_EINVAL, "panns_set_base: base has " + std::to_string(n) +
+                                      " vectors, the graph has " + std::to_string(h->gn) + " vertices");
     CU(cudaSetDevice(h->device));
-    int rc = upload_chain_major(h, data, n, d, h->vec);
-    if (rc) return rc;
+    CU(h->base_raw.ensure((size_t) n * d));
+    CU(cudaMemcpyAsync(h->base_raw.p, data, (size_t) n * d * sizeof(float), cudaMemcpyHostToDevice,
+                       h->stream));
+    CU(cudaStreamSynchronize(h->stream));
     h->n = n;
     h->d = d;
     h->dpad = ((d + 31) / 32) * 32;
     h->storage = storage;
-    CU(h->norms.ensure(n));
-    const int blocks = std::max(1, (int) std::min<uint32_t>((n + 255) / 256, h->num_sms * 32u));
-    norms_kernel<<<blocks, 256, 0, h->stream>>>(h->vec.p, h->norms.p, n, (int) h->dpad);
-    CU(cudaGetLastError());
-    CU(cudaStreamSynchronize(h->stream));
-    h->raw.release();
+    h->ready = false;
     return PANNS_OK;
 }
 
@@ -292,21 +335,83 @@ int panns_set_graph(panns_index *h, uint32_t width, uint32_t entry, const uint64
         if (nbrs[e] >= n)
             return fail(PANNS_EINVAL, "panns_set_graph: neighbour id " + std::to_string(nbrs[e]) +
                                           " >= N");
-    CU(cudaSetDevice(h->device));
     h->off.assign(offsets, offsets + n + 1);
     h->nbrs.assign(nbrs, nbrs + E);
+    h->width = width;
+    h->entry = entry;
+    h->gn = n;
+    h->ready = false;
+    return PANNS_OK;
+}
+
+// Build the search layout from the current base + graph: the locality order
+// (vertices grouped by their nearest of C pivot vertices, original id order
+// inside a group), chain-major rows and norms in that order, head rows and
+// overflow lists in device ids.
+static int finalize(panns_index *h) {
+    if (h->ready) return PANNS_OK;
+    if (!h->n || !h->base_raw.p) return fail(PANNS_ESTATE, "search: no base vectors loaded");
+    if (!h->gn) return fail(PANNS_ESTATE, "search: no graph loaded");
+    if (h->gn != h->n) return fail(PANNS_ESTATE, "search: graph and base sizes differ");
+    const uint32_t n = h->n;
+    CU(cudaSetDevice(h->device));
+    h->perm.resize(n);
+    h->inv.resize(n);
+    const char *ord = getenv("PANNS_LAYOUT_ORDER");
+    const bool identity = (ord && std::string(ord) == "identity") || n < 4096;
+    if (identity) {
+        for (uint32_t v = 0; v < n; ++v) h->perm[v] = h->inv[v] = v;
+    } else {
+        const uint32_t C = std::max(1u, std::min(4096u, n / 256));
+        std::vector<uint32_t> piv(C), cell(n);
+        for (uint32_t p = 0; p < C; ++p) piv[p] = (uint32_t) (((uint64_t) p * n) / C);
+        DevBuf<uint32_t> dpiv, dcell;
+        CU(dpiv.ensure(C));
+        CU(dcell.ensure(n));
+        CU(cudaMemcpyAsync(dpiv.p, piv.data(), C * 4ull, cudaMemcpyHostToDevice, h->stream));
+        nearest_pivot_kernel<<<h->num_sms * 8, 256, 0, h->stream>>>(h->base_raw.p, n, (int) h->d, dpiv.p,
+                                                                    C, dcell.p);
+        CU(cudaGetLastError());
+        CU(cudaMemcpyAsync(cell.data(), dcell.p, n * 4ull, cudaMemcpyDeviceToHost, h->stream));
+        CU(cudaStreamSynchronize(h->stream));
+        std::vector<uint32_t> start(C + 1, 0);
+        for (uint32_t v = 0; v < n; ++v) start[cell[v] + 1]++;
+        for (uint32_t c = 0; c < C; ++c) start[c + 1] += start[c];
+        for (uint32_t v = 0; v < n; ++v) h->perm[start[cell[v]]++] = v;
+        for (uint32_t u = 0; u < n; ++u) h->inv[h->perm[u]] = u;
+    }
+    CU(h->orig.ensure(n));
+    CU(cudaMemcpyAsync(h->orig.p, h->perm.data(), n * 4ull, cudaMemcpyHostToDevice, h->stream));
+    // rows and norms
+    CU(h->vec.ensure((size_t) n * h->dpad));
+    {
+        const uint64_t total = (uint64_t) n * h->dpad;
+        const int blocks = (int) std::min<uint64_t>((total + 255) / 256, (uint64_t) h->num_sms * 32);
+        permute_rows_kernel<<<std::max(blocks, 1), 256, 0, h->stream>>>(h->base_raw.p, h->vec.p, n,
+                                                                       (int) h->d, (int) h->dpad,
+                                                                       h->orig.p);
+        CU(cudaGetLastError());
+    }
+    CU(h->norms.ensure(n));
+    {
+        const int blocks = std::max(1, (int) std::min<uint32_t>((n + 255) / 256, h->num_sms * 32u));
+        norms_kernel<<<blocks, 256, 0, h->stream>>>(h->vec.p, h->norms.p, n, (int) h->dpad);
+        CU(cudaGetLastError());
+    }
+    // head rows + overflow in device ids
     std::vector<uint32_t> head((size_t) n * kHeadWords, 0u);
     std::vector<uint64_t> ovf_off(n, 0);
     std::vector<uint32_t> ovf;
-    for (uint32_t v = 0; v < n; ++v) {
-        const uint64_t deg = offsets[v + 1] - offsets[v];
-        uint32_t *row = head.data() + (size_t) v * kHeadWords;
+    for (uint32_t u = 0; u < n; ++u) {
+        const uint32_t v = h->perm[u];
+        const uint64_t b = h->off[v], deg = h->off[v + 1] - b;
+        uint32_t *row = head.data() + (size_t) u * kHeadWords;
         row[0] = (uint32_t) deg;
         const uint64_t h1 = std::min<uint64_t>(deg, kHeadNbrs);
-        for (uint64_t s = 0; s < h1; ++s) row[1 + s] = nbrs[offsets[v] + s];
+        for (uint64_t s2 = 0; s2 < h1; ++s2) row[1 + s2] = h->inv[h->nbrs[b + s2]];
         if (deg > (uint64_t) kHeadNbrs) {
-            ovf_off[v] = ovf.size();
-            ovf.insert(ovf.end(), nbrs + offsets[v] + kHeadNbrs, nbrs + offsets[v + 1]);
+            ovf_off[u] = ovf.size();
+            for (uint64_t s2 = kHeadNbrs; s2 < deg; ++s2) ovf.push_back(h->inv[h->nbrs[b + s2]]);
         }
     }
     CU(h->head.ensure(head.size()));
@@ -317,9 +422,7 @@ int panns_set_graph(panns_index *h, uint32_t width, uint32_t entry, const uint64
     if (!ovf.empty())
         CU(cudaMemcpyAsync(h->ovf.p, ovf.data(), ovf.size() * 4, cudaMemcpyHostToDevice, h->stream));
     CU(cudaStreamSynchronize(h->stream));
-    h->width = width;
-    h->entry = entry;
-    h->gn = n;
+    h->ready = true;
     return PANNS_OK;
 }
 
@@ -476,11 +579,10 @@ const void *kernel_for(uint32_t kind, uint32_t order, int CL) {
                                 : pick_kernel<KIND_L2, ORDER_EFANNA>(CL);
 }
 
-int check_params(const panns_index *h, const panns_search_params *p) {
+int check_params(panns_index *h, const panns_search_params *p) {
     if (!p) return fail(PANNS_EINVAL, "search: NULL params");
-    if (!h->n || !h->vec.p) return fail(PANNS_ESTATE, "search: no base vectors loaded");
-    if (!h->gn || !h->head.p) return fail(PANNS_ESTATE, "search: no graph loaded");
-    if (h->gn != h->n) return fail(PANNS_ESTATE, "search: graph and base sizes differ");
+    int rc = finalize(h);
+    if (rc) return rc;
     if (p->mode > PANNS_MODE_EFANNA) return fail(PANNS_EINVAL, "search: unknown mode");
     if (p->distance > PANNS_DIST_L2) return fail(PANNS_EINVAL, "search: unknown distance");
     if (p->L == 0 || p->L > h->n) return fail(PANNS_EINVAL, "search: need 0 < L <= N");
@@ -548,6 +650,7 @@ static int launch_search(panns_index *h, const panns_search_params *p, const flo
     a.head = h->head.p;
     a.ovf_off = h->ovf_off.p;
     a.ovf = h->ovf.p;
+    a.orig = h->orig.p;
     a.n = h->n;
     a.queries = reinterpret_cast<const float4 *>(d_queries_cm);
     a.nq = nq;
@@ -601,18 +704,23 @@ static int resolve_init(panns_index *h, const panns_search_params *p, const uint
             ids = buf.data();
         }
     }
-    // Init ids must be valid, distinct vertices (per query).
+    // Init ids must be valid, distinct vertices (per query); they are handed
+    // to the kernel as device ids, in the same order.
     const uint32_t groups = stride ? nq : 1;
     std::vector<uint8_t> seen(h->n, 0);
+    std::vector<uint32_t> dev((size_t) groups * L);
     for (uint32_t g = 0; g < groups; ++g) {
         const uint32_t *x = ids + (size_t) g * L;
         for (uint32_t i = 0; i < L; ++i) {
             if (x[i] >= h->n) return fail(PANNS_EINVAL, "search: init id out of range");
             if (seen[x[i]]) return fail(PANNS_EINVAL, "search: duplicate init id");
             seen[x[i]] = 1;
+            dev[(size_t) g * L + i] = h->inv[x[i]];
         }
         for (uint32_t i = 0; i < L; ++i) seen[x[i]] = 0;
     }
+    buf.swap(dev);
+    ids = buf.data();
     return PANNS_OK;
 }
 

@@ -20,14 +20,21 @@
 // all fresh distances of the step at once, sorts the survivors and merges
 // them in one rank-based pass; chunked merges give the same result.
 //
-// HBM layout (built by layout kernels in panns_abi.cu):
+// Vertex numbering on the device: vertices are stored in a locality order
+// (see panns_abi.cu), so a query's visited bits and gathers cluster. The
+// kernel works on these device ids; `orig` maps them back. Original ids are
+// used wherever the reference's semantics depend on ids: the (dist, id)
+// tie-break (looked up only when two distances are exactly equal) and the
+// output.
+//
+// HBM layout (built in panns_abi.cu):
 //   vec   n x (CL*8) float4, "chain-major": float4 number 8*i + c of a row holds
 //         terms 4i..4i+3 of lane accumulator c of the reference's 8-lane
 //         distance loop, so the 8 threads of a vertex read one 128-byte line
 //         per load and each thread runs its lane's FMA chain in the reference
 //         order. Padding terms are zero (an FMA with 0*0 leaves a lane as is).
 //   norm  n float32, ||v||^2 in the same lane order (norm-trick distance).
-//   head  n x 16 u32: degree, then the first 15 neighbour ids (one 64-byte
+//   head  n x 32 u32: degree, then the first 31 neighbour ids (one 128-byte
 //         read per expansion); ovf_off/ovf: the rest of longer rows (CSR).
 //
 // Per warp (shared memory): the queue (L x (dist f32, id u32 with bit 31 =
@@ -44,10 +51,11 @@ namespace panns {
 constexpr uint32_t kChecked = 0x80000000u;
 constexpr uint32_t kIdMask = 0x7fffffffu;
 constexpr uint32_t kFull = 0xffffffffu;
-constexpr int kHeadWords = 16;   // degree + 15 neighbours
+constexpr int kHeadWords = 32;   // degree + 31 neighbours
 constexpr int kHeadNbrs = kHeadWords - 1;
 constexpr int kBuf = 256;        // fresh-candidate buffer per warp
-constexpr int kCandGroup = 16;   // candidates whose head rows are staged at once
+constexpr int kCandGroup = 8;    // candidates whose head rows are staged at once
+constexpr int kGroupChunks = (kCandGroup * kHeadNbrs + 31) / 32;
 constexpr int kMaxM = 64;
 
 enum { ORDER_PANNS = 0, ORDER_EFANNA = 1 };
@@ -59,16 +67,17 @@ enum : uint32_t { ERR_BAD_ID = 1u, ERR_BAD_INIT = 2u };
 struct SearchArgs {
     const float4 *vec;        // n x (CL*8) float4
     const float *norms;       // n (KIND_IP)
-    const uint32_t *head;     // n x 16
+    const uint32_t *head;     // n x 32
     const uint64_t *ovf_off;  // n
     const uint32_t *ovf;      // overflow neighbours
+    const uint32_t *orig;     // device id -> original id
     uint32_t n;
     const float4 *queries;    // nq x (CL*8) float4, chain-major
     uint32_t nq;
-    const uint32_t *init_ids; // L ids, or nq x L when init_stride == L
+    const uint32_t *init_ids; // L device ids, or nq x L when init_stride == L
     uint32_t init_stride;
     uint32_t K, L, M;
-    uint32_t *out_ids;        // nq x K
+    uint32_t *out_ids;        // nq x K original ids
     uint4 *out_stats;         // nq x {n_dist, n_expand, n_edges, n_iter}
     uint32_t *visited;        // slots x vis_words
     uint32_t vis_words;
@@ -119,65 +128,97 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
 }
 
 // ---------------------------------------------------------------------------
-// Distance of one vertex, computed by the 8 lanes of a group (c = lane & 7 is
-// the lane accumulator this thread owns). Every lane of the group returns it.
+// Distances of two vertices per 8-lane group (c = lane & 7 is the lane
+// accumulator this thread owns): both rows are loaded before either is used.
 // Lane sum: ((u0 + u1) + u2) + ... + u7; norm trick: -2 * dot + norm, which
 // is one rounding either way because -2 * dot is exact.
 // ---------------------------------------------------------------------------
 template <int KIND, int CL>
-__device__ __forceinline__ float group_distance(const float4 *__restrict__ vec,
-                                                const float *__restrict__ norms, uint32_t v,
-                                                bool active, const float4 (&qv)[CL], int lane) {
-    const int c = lane & 7;
+__device__ __forceinline__ float chain(const float4 (&x)[CL], const float4 (&qv)[CL]) {
     float acc = 0.0f;
-    float nrm = 0.0f;
-    if (active) {
-        const float4 *row = vec + (size_t) v * (CL * 8);
-        float4 x[CL];
 #pragma unroll
-        for (int i = 0; i < CL; ++i) x[i] = __ldg(row + 8 * i + c);
-        if (KIND == KIND_IP) nrm = __ldg(norms + v);
-#pragma unroll
-        for (int i = 0; i < CL; ++i) {
-            if (KIND == KIND_IP) {
-                acc = __fmaf_rn(x[i].x, qv[i].x, acc);
-                acc = __fmaf_rn(x[i].y, qv[i].y, acc);
-                acc = __fmaf_rn(x[i].z, qv[i].z, acc);
-                acc = __fmaf_rn(x[i].w, qv[i].w, acc);
-            } else {
-                float t;
-                t = __fsub_rn(x[i].x, qv[i].x); acc = __fmaf_rn(t, t, acc);
-                t = __fsub_rn(x[i].y, qv[i].y); acc = __fmaf_rn(t, t, acc);
-                t = __fsub_rn(x[i].z, qv[i].z); acc = __fmaf_rn(t, t, acc);
-                t = __fsub_rn(x[i].w, qv[i].w); acc = __fmaf_rn(t, t, acc);
-            }
+    for (int i = 0; i < CL; ++i) {
+        if (KIND == KIND_IP) {
+            acc = __fmaf_rn(x[i].x, qv[i].x, acc);
+            acc = __fmaf_rn(x[i].y, qv[i].y, acc);
+            acc = __fmaf_rn(x[i].z, qv[i].z, acc);
+            acc = __fmaf_rn(x[i].w, qv[i].w, acc);
+        } else {
+            float t;
+            t = __fsub_rn(x[i].x, qv[i].x); acc = __fmaf_rn(t, t, acc);
+            t = __fsub_rn(x[i].y, qv[i].y); acc = __fmaf_rn(t, t, acc);
+            t = __fsub_rn(x[i].z, qv[i].z); acc = __fmaf_rn(t, t, acc);
+            t = __fsub_rn(x[i].w, qv[i].w); acc = __fmaf_rn(t, t, acc);
         }
     }
+    return acc;
+}
+
+__device__ __forceinline__ float lane_sum8(float acc, int lane) {
     const int base = lane & ~7;
     float s = __shfl_sync(kFull, acc, base);
 #pragma unroll
     for (int j = 1; j < 8; ++j) s = __fadd_rn(s, __shfl_sync(kFull, acc, base + j));
-    if (KIND == KIND_IP) s = __fmaf_rn(-2.0f, s, nrm);
     return s;
 }
 
-__device__ __forceinline__ bool key_less(float ad, uint32_t ak, float bd, uint32_t bk) {
-    return ad < bd || (ad == bd && ak < bk);
+template <int KIND, int CL>
+__device__ __forceinline__ void group_distance2(const float4 *__restrict__ vec,
+                                                const float *__restrict__ norms, uint32_t v0,
+                                                bool a0, uint32_t v1, bool a1,
+                                                const float4 (&qv)[CL], int lane, float &d0,
+                                                float &d1) {
+    const int c = lane & 7;
+    float4 x0[CL], x1[CL];
+    float n0 = 0.f, n1 = 0.f;
+    const float4 *r0 = vec + (size_t) v0 * (CL * 8) + c;
+    const float4 *r1 = vec + (size_t) v1 * (CL * 8) + c;
+#pragma unroll
+    for (int i = 0; i < CL; ++i) {
+        x0[i] = a0 ? __ldg(r0 + 8 * i) : make_float4(0.f, 0.f, 0.f, 0.f);
+        x1[i] = a1 ? __ldg(r1 + 8 * i) : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    if (KIND == KIND_IP) {
+        n0 = a0 ? __ldg(norms + v0) : 0.f;
+        n1 = a1 ? __ldg(norms + v1) : 0.f;
+    }
+    float s0 = lane_sum8(chain<KIND, CL>(x0, qv), lane);
+    float s1 = lane_sum8(chain<KIND, CL>(x1, qv), lane);
+    if (KIND == KIND_IP) {
+        s0 = __fmaf_rn(-2.0f, s0, n0);
+        s1 = __fmaf_rn(-2.0f, s1, n1);
+    }
+    d0 = s0;
+    d1 = s1;
+}
+
+// (dist, key) order. PANNS: key is a device id and equal distances compare
+// original ids; EFANNA: key is the arrival index.
+template <int ORDER>
+__device__ __forceinline__ bool key_less(float ad, uint32_t ak, float bd, uint32_t bk,
+                                         const uint32_t *__restrict__ orig) {
+    if (ad != bd) return ad < bd;
+    if (ORDER == ORDER_PANNS) {
+        if (ak == bk) return false;
+        if (ak == kFull || bk == kFull) return ak < bk;  // padding sorts last
+        return __ldg(orig + ak) < __ldg(orig + bk);
+    }
+    return ak < bk;
 }
 
 // Number of queue elements that precede a fresh element (d, id).
 template <int ORDER>
 __device__ __forceinline__ uint32_t queue_rank(const float *qd, const uint32_t *qi, uint32_t sz,
-                                               float d, uint32_t id) {
+                                               float d, uint32_t id, const uint32_t *orig) {
     uint32_t lo = 0, hi = sz;
     while (lo < hi) {
         uint32_t mid = (lo + hi) >> 1;
+        const float md = qd[mid];
         bool before;
         if (ORDER == ORDER_PANNS) {
-            float md = qd[mid];
-            before = md < d || (md == d && (qi[mid] & kIdMask) < id);
+            before = md < d || (md == d && __ldg(orig + (qi[mid] & kIdMask)) < __ldg(orig + id));
         } else {
-            before = qd[mid] <= d;  // older elements stay ahead of equal distances
+            before = md <= d;  // older elements stay ahead of equal distances
         }
         if (before) lo = mid + 1; else hi = mid;
     }
@@ -187,28 +228,63 @@ __device__ __forceinline__ uint32_t queue_rank(const float *qd, const uint32_t *
 // Number of sorted fresh elements that precede a queue element (d, id).
 template <int ORDER>
 __device__ __forceinline__ uint32_t fresh_rank(const float *bd, const uint32_t *bi, uint32_t cnt,
-                                               float d, uint32_t id) {
+                                               float d, uint32_t id, const uint32_t *orig) {
     uint32_t lo = 0, hi = cnt;
     while (lo < hi) {
         uint32_t mid = (lo + hi) >> 1;
+        const float md = bd[mid];
         bool before;
         if (ORDER == ORDER_PANNS) {
-            float md = bd[mid];
-            before = md < d || (md == d && bi[mid] < id);
+            before = md < d || (md == d && __ldg(orig + bi[mid]) < __ldg(orig + id));
         } else {
-            before = bd[mid] < d;
+            before = md < d;
         }
         if (before) lo = mid + 1; else hi = mid;
     }
     return lo;
 }
 
-// Bitonic sort of (bd, bk)[0..cnt) by (dist, key), carrying bi along when
-// carry_ids; the padding up to the next power of two holds (+inf, ~0).
-__device__ void warp_sort(float *bd, uint32_t *bi, uint32_t *bk, uint32_t cnt, bool carry_ids,
-                          int lane) {
+// Sort (bd, bk, bi)[0..cnt) by (dist, key). Up to 32 elements: a bitonic
+// network across the lanes in registers; more: a bitonic network in shared
+// memory (padding up to the next power of two holds (+inf, ~0)).
+template <int ORDER>
+__device__ void warp_sort(float *bd, uint32_t *bi, uint32_t *bk, uint32_t cnt,
+                          const uint32_t *orig, int lane) {
     if (cnt <= 1) return;
-    uint32_t n = 1;
+    if (cnt <= 32) {
+        const bool have = (uint32_t) lane < cnt;
+        float d = have ? bd[lane] : __int_as_float(0x7f800000);
+        uint32_t k = have ? bk[lane] : kFull;
+        uint32_t id = have ? bi[lane] : kFull;
+#pragma unroll
+        for (int kk = 2; kk <= 32; kk <<= 1) {
+#pragma unroll
+            for (int j = kk >> 1; j > 0; j >>= 1) {
+                const float pd = __shfl_xor_sync(kFull, d, j);
+                const uint32_t pk = __shfl_xor_sync(kFull, k, j);
+                const uint32_t pid = __shfl_xor_sync(kFull, id, j);
+                const bool up = (lane & kk) == 0;
+                const bool lower = (lane & j) == 0;
+                const bool p_less = key_less<ORDER>(pd, pk, d, k, orig);
+                const bool me_less = key_less<ORDER>(d, k, pd, pk, orig);
+                const bool take = (lower == up) ? p_less : me_less;
+                if (take) {
+                    d = pd;
+                    k = pk;
+                    id = pid;
+                }
+            }
+        }
+        __syncwarp();
+        if (have) {
+            bd[lane] = d;
+            bk[lane] = k;
+            bi[lane] = id;
+        }
+        __syncwarp();
+        return;
+    }
+    uint32_t n = 64;
     while (n < cnt) n <<= 1;
     for (uint32_t i = cnt + lane; i < n; i += 32) {
         bd[i] = __int_as_float(0x7f800000);
@@ -219,16 +295,17 @@ __device__ void warp_sort(float *bd, uint32_t *bi, uint32_t *bk, uint32_t cnt, b
     for (uint32_t k = 2; k <= n; k <<= 1) {
         for (uint32_t j = k >> 1; j > 0; j >>= 1) {
             for (uint32_t i = lane; i < n; i += 32) {
-                uint32_t ixj = i ^ j;
+                const uint32_t ixj = i ^ j;
                 if (ixj > i) {
-                    float ad = bd[i], xd = bd[ixj];
-                    uint32_t ak = bk[i], xk = bk[ixj];
-                    bool up = (i & k) == 0;
-                    bool sw = up ? key_less(xd, xk, ad, ak) : key_less(ad, ak, xd, xk);
+                    const float ad = bd[i], xd = bd[ixj];
+                    const uint32_t ak = bk[i], xk = bk[ixj];
+                    const bool up = (i & k) == 0;
+                    const bool sw = up ? key_less<ORDER>(xd, xk, ad, ak, orig)
+                                       : key_less<ORDER>(ad, ak, xd, xk, orig);
                     if (sw) {
                         bd[i] = xd; bd[ixj] = ad;
                         bk[i] = xk; bk[ixj] = ak;
-                        if (carry_ids) { uint32_t t = bi[i]; bi[i] = bi[ixj]; bi[ixj] = t; }
+                        const uint32_t t = bi[i]; bi[i] = bi[ixj]; bi[ixj] = t;
                     }
                 }
             }
@@ -241,12 +318,13 @@ __device__ void warp_sort(float *bd, uint32_t *bi, uint32_t *bk, uint32_t cnt, b
 // (capacity L). Returns the position of the first fresh element if it was
 // inserted (< L), else L. Uses bk as scratch.
 template <int ORDER>
-__device__ uint32_t warp_merge(const WarpMem &m, uint32_t *sz, uint32_t L, uint32_t cnt, int lane) {
+__device__ uint32_t warp_merge(const WarpMem &m, uint32_t *sz, uint32_t L, uint32_t cnt,
+                               const uint32_t *orig, int lane) {
     const uint32_t qsz = *sz;
     if (cnt == 0) return L;
     // Merged position of each fresh element: its index plus its rank in the old queue.
     for (uint32_t i = lane; i < cnt; i += 32)
-        m.bk[i] = i + queue_rank<ORDER>(m.qd, m.qi, qsz, m.bd[i], m.bi[i]);
+        m.bk[i] = i + queue_rank<ORDER>(m.qd, m.qi, qsz, m.bd[i], m.bi[i], orig);
     __syncwarp();
     const uint32_t p0 = m.bk[0];
     if (p0 >= L) return L;
@@ -259,7 +337,7 @@ __device__ uint32_t warp_merge(const WarpMem &m, uint32_t *sz, uint32_t L, uint3
         if (j >= (int32_t) p0) {
             d = m.qd[j];
             id = m.qi[j];
-            np = (uint32_t) j + fresh_rank<ORDER>(m.bd, m.bi, cnt, d, id & kIdMask);
+            np = (uint32_t) j + fresh_rank<ORDER>(m.bd, m.bi, cnt, d, id & kIdMask, orig);
         }
         __syncwarp();
         if (np < L) {
@@ -280,26 +358,21 @@ __device__ uint32_t warp_merge(const WarpMem &m, uint32_t *sz, uint32_t L, uint3
     return p0;
 }
 
-// Visited test-and-set on the slot's bitset; records words that went from 0.
-// Returns true for a vertex not seen before in this query.
-__device__ __forceinline__ bool visit(uint32_t *vis, uint32_t *dirty, uint32_t dirty_cap,
-                                      uint32_t &dcount, uint32_t id, bool valid, int lane) {
-    bool fresh = false, first = false;
-    uint32_t w = 0;
-    if (valid) {
-        w = id >> 5;
-        const uint32_t bit = 1u << (id & 31);
-        const uint32_t old = atomicOr(vis + w, bit);
-        fresh = (old & bit) == 0;
-        first = old == 0;
-    }
+// Visited bitset: test-and-set returns the previous word.
+__device__ __forceinline__ uint32_t visit_issue(uint32_t *vis, uint32_t id, bool valid) {
+    return valid ? atomicOr(vis + (id >> 5), 1u << (id & 31)) : kFull;
+}
+
+// Record the words that went from zero to non-zero (only those are cleared
+// after the query).
+__device__ __forceinline__ void note_dirty(uint32_t *dirty, uint32_t dirty_cap, uint32_t &dcount,
+                                           bool first, uint32_t word) {
     const uint32_t bm = __ballot_sync(kFull, first);
     if (first) {
         const uint32_t pos = dcount + __popc(bm & lanemask_lt());
-        if (pos < dirty_cap) dirty[pos] = w;
+        if (pos < dirty_cap) dirty[pos] = word;
     }
     dcount += __popc(bm);
-    return fresh;
 }
 
 // Compute distances of the buffered fresh vertices bi[0..nb), keep the ones
@@ -309,18 +382,23 @@ template <int KIND, int ORDER, int CL>
 __device__ uint32_t flush(const SearchArgs &a, const WarpMem &m, uint32_t nb, uint32_t *sz,
                           bool filter, const float4 (&qv)[CL], int lane) {
     const int g = lane >> 3;
-    // Distances, 4 vertices per pass (8 lanes each).
-    for (uint32_t b0 = 0; b0 < nb; b0 += 4) {
-        const uint32_t b = b0 + g;
-        const bool act = b < nb;
-        const uint32_t v = act ? m.bi[b] : 0u;
-        const float dist = group_distance<KIND, CL>(a.vec, a.norms, v, act, qv, lane);
-        if (act && (lane & 7) == 0) m.bd[b] = dist;
+    // Distances, 8 vertices per round (2 per 8-lane group, loads issued together).
+    for (uint32_t b0 = 0; b0 < nb; b0 += 8) {
+        const uint32_t b = b0 + g, bb = b0 + 4 + g;
+        const bool act0 = b < nb, act1 = bb < nb;
+        const uint32_t v0 = act0 ? m.bi[b] : 0u, v1 = act1 ? m.bi[bb] : 0u;
+        float d0, d1;
+        group_distance2<KIND, CL>(a.vec, a.norms, v0, act0, v1, act1, qv, lane, d0, d1);
+        if ((lane & 7) == 0) {
+            if (act0) m.bd[b] = d0;
+            if (act1) m.bd[bb] = d1;
+        }
     }
     __syncwarp();
     // Keep the survivors, in arrival order.
     const uint32_t L = a.L;
     const float bound = (filter && *sz >= L) ? m.qd[L - 1] : __int_as_float(0x7f800000);
+    const bool any_bound = filter && *sz >= L;
     uint32_t cnt = 0;
     for (uint32_t b0 = 0; b0 < nb; b0 += 32) {
         const uint32_t b = b0 + lane;
@@ -330,7 +408,7 @@ __device__ uint32_t flush(const SearchArgs &a, const WarpMem &m, uint32_t nb, ui
         if (b < nb) {
             d = m.bd[b];
             id = m.bi[b];
-            keep = !filter || *sz < L || (ORDER == ORDER_PANNS ? !(d > bound) : d < bound);
+            keep = !any_bound || (ORDER == ORDER_PANNS ? !(d > bound) : d < bound);
         }
         const uint32_t bm = __ballot_sync(kFull, keep);
         __syncwarp();
@@ -344,8 +422,26 @@ __device__ uint32_t flush(const SearchArgs &a, const WarpMem &m, uint32_t nb, ui
         __syncwarp();
     }
     if (cnt == 0) return L;
-    warp_sort(m.bd, m.bi, m.bk, cnt, true, lane);
-    return warp_merge<ORDER>(m, sz, L, cnt, lane);
+    warp_sort<ORDER>(m.bd, m.bi, m.bk, cnt, a.orig, lane);
+    return warp_merge<ORDER>(m, sz, L, cnt, a.orig, lane);
+}
+
+// Append this lane's fresh vertex (if any) to the buffer, flushing first when
+// a full chunk might not fit.
+template <int KIND, int ORDER, int CL>
+__device__ __forceinline__ void append_fresh(const SearchArgs &a, const WarpMem &m, uint32_t &nb,
+                                             uint32_t *sz, uint32_t &nk, uint32_t &n_dist,
+                                             bool fresh, uint32_t id, const float4 (&qv)[CL],
+                                             int lane) {
+    if (nb + 32 > kBuf) {
+        n_dist += nb;
+        nk = min(nk, flush<KIND, ORDER, CL>(a, m, nb, sz, true, qv, lane));
+        nb = 0;
+    }
+    const uint32_t bm = __ballot_sync(kFull, fresh);
+    if (fresh) m.bi[nb + __popc(bm & lanemask_lt())] = id;
+    nb += __popc(bm);
+    __syncwarp();
 }
 
 // One query, run by one warp.
@@ -371,9 +467,10 @@ __device__ void search_one(const SearchArgs &a, const WarpMem &m, uint32_t q, ui
         const uint32_t i = i0 + lane;
         const bool valid = i < L;
         uint32_t id = valid ? __ldg(init + i) : 0u;
-        bool ok = valid && id < a.n;
+        const bool ok = valid && id < a.n;
         if (valid && !ok) atomicOr(a.error, ERR_BAD_INIT);
-        visit(vis, dirty, a.dirty_cap, dcount, id, ok, lane);
+        const uint32_t old = visit_issue(vis, id, ok);
+        note_dirty(dirty, a.dirty_cap, dcount, ok && old == 0, id >> 5);
         const uint32_t bm = __ballot_sync(kFull, ok);
         if (ok) m.bi[nb + __popc(bm & lanemask_lt())] = id;
         nb += __popc(bm);
@@ -400,10 +497,13 @@ __device__ void search_one(const SearchArgs &a, const WarpMem &m, uint32_t q, ui
                 const uint32_t id = m.qi[p];
                 m.qi[p] = id | kChecked;
                 m.cand[cnt + r] = id;
-                if (r == take - 1) m.pre[63] = p;
             }
-            __syncwarp();
-            if (take) last_k = m.pre[63];
+            if (take) {
+                // position of the take-th unchecked slot in this window
+                uint32_t x = bm;
+                for (uint32_t t = 1; t < take; ++t) x &= x - 1;
+                last_k = p0 + (__ffs(x) - 1);
+            }
             cnt += take;
             __syncwarp();
         }
@@ -414,21 +514,17 @@ __device__ void search_one(const SearchArgs &a, const WarpMem &m, uint32_t q, ui
         nb = 0;
         for (uint32_t c0 = 0; c0 < cnt; c0 += kCandGroup) {
             const uint32_t gc = min((uint32_t) kCandGroup, cnt - c0);
-            // Stage the head rows: 2 candidates per warp-wide load, all loads
-            // issued before the first store.
+            // Stage the head rows: one warp-wide 128-byte load per candidate,
+            // all issued before the first store.
             {
-                uint32_t hv[kCandGroup / 2];
+                uint32_t hv[kCandGroup];
 #pragma unroll
-                for (int r = 0; r < kCandGroup / 2; ++r) {
-                    const uint32_t j = 2 * r + (lane >> 4);
-                    hv[r] = j < gc ? __ldg(a.head + (size_t) m.cand[c0 + j] * kHeadWords + (lane & 15))
-                                   : 0u;
-                }
+                for (int j = 0; j < kCandGroup; ++j)
+                    hv[j] = (uint32_t) j < gc ? __ldg(a.head + (size_t) m.cand[c0 + j] * kHeadWords + lane)
+                                              : 0u;
 #pragma unroll
-                for (int r = 0; r < kCandGroup / 2; ++r) {
-                    const uint32_t j = 2 * r + (lane >> 4);
-                    if (j < gc) m.hrow[j * kHeadWords + (lane & 15)] = hv[r];
-                }
+                for (int j = 0; j < kCandGroup; ++j)
+                    if ((uint32_t) j < gc) m.hrow[j * kHeadWords + lane] = hv[j];
             }
             __syncwarp();
             // Prefix sums of the head-row neighbour counts.
@@ -449,12 +545,16 @@ __device__ void search_one(const SearchArgs &a, const WarpMem &m, uint32_t q, ui
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) degsum += __shfl_xor_sync(kFull, degsum, o);
             n_edges += gc + degsum;
+            const bool any_long = __any_sync(kFull, deg > (uint32_t) kHeadNbrs);
             __syncwarp();
-            // Head-row neighbours, in (candidate, slot) order.
-            for (uint32_t f0 = 0; f0 < total; f0 += 32) {
-                const uint32_t f = f0 + lane;
-                bool valid = f < total;
+            // Head-row neighbours in (candidate, slot) order: every visited
+            // test-and-set of the group is issued before any result is used.
+            uint32_t ids[kGroupChunks], olds[kGroupChunks];
+#pragma unroll
+            for (int ch = 0; ch < kGroupChunks; ++ch) {
+                const uint32_t f = ch * 32 + lane;
                 uint32_t id = 0;
+                bool valid = f < total;
                 if (valid) {
                     uint32_t j = 0;
                     while (j + 1 < gc && m.pre[j + 1] <= f) ++j;
@@ -464,57 +564,52 @@ __device__ void search_one(const SearchArgs &a, const WarpMem &m, uint32_t q, ui
                         valid = false;
                     }
                 }
-                const bool fresh = visit(vis, dirty, a.dirty_cap, dcount, id, valid, lane);
-                if (nb + 32 > kBuf) {
-                    n_dist += nb;
-                    const uint32_t r = flush<KIND, ORDER, CL>(a, m, nb, &sz, true, qv, lane);
-                    nk = min(nk, r);
-                    nb = 0;
-                }
-                const uint32_t bm = __ballot_sync(kFull, fresh);
-                if (fresh) m.bi[nb + __popc(bm & lanemask_lt())] = id;
-                nb += __popc(bm);
-                __syncwarp();
+                ids[ch] = valid ? id : kFull;
+                olds[ch] = visit_issue(vis, id, valid);
             }
-            // Rows longer than the head: the rest from the overflow list.
-            for (uint32_t j = 0; j < gc; ++j) {
-                const uint32_t dj = m.hrow[j * kHeadWords];
-                if (dj <= (uint32_t) kHeadNbrs) continue;
-                const uint64_t off = __ldg(a.ovf_off + m.cand[c0 + j]);
-                for (uint32_t s0 = kHeadNbrs; s0 < dj; s0 += 32) {
-                    const uint32_t s = s0 + lane;
-                    bool valid = s < dj;
-                    uint32_t id = valid ? __ldg(a.ovf + off + (s - kHeadNbrs)) : 0u;
-                    if (valid && id >= a.n) {
-                        atomicOr(a.error, ERR_BAD_ID);
-                        valid = false;
+#pragma unroll
+            for (int ch = 0; ch < kGroupChunks; ++ch) {
+                if (ch * 32 >= (int) total) break;
+                const uint32_t id = ids[ch];
+                const bool valid = id != kFull;
+                const bool fresh = valid && !(olds[ch] & (1u << (id & 31)));
+                note_dirty(dirty, a.dirty_cap, dcount, valid && olds[ch] == 0, id >> 5);
+                append_fresh<KIND, ORDER, CL>(a, m, nb, &sz, nk, n_dist, fresh, id, qv, lane);
+            }
+            // Rows longer than the head row: the rest from the overflow list.
+            if (any_long) {
+                for (uint32_t j = 0; j < gc; ++j) {
+                    const uint32_t dj = m.hrow[j * kHeadWords];
+                    if (dj <= (uint32_t) kHeadNbrs) continue;
+                    const uint64_t off = __ldg(a.ovf_off + m.cand[c0 + j]);
+                    for (uint32_t s0 = kHeadNbrs; s0 < dj; s0 += 32) {
+                        const uint32_t s = s0 + lane;
+                        bool valid = s < dj;
+                        const uint32_t id = valid ? __ldg(a.ovf + off + (s - kHeadNbrs)) : 0u;
+                        if (valid && id >= a.n) {
+                            atomicOr(a.error, ERR_BAD_ID);
+                            valid = false;
+                        }
+                        const uint32_t old = visit_issue(vis, id, valid);
+                        const bool fresh = valid && !(old & (1u << (id & 31)));
+                        note_dirty(dirty, a.dirty_cap, dcount, valid && old == 0, id >> 5);
+                        append_fresh<KIND, ORDER, CL>(a, m, nb, &sz, nk, n_dist, fresh, id, qv, lane);
                     }
-                    const bool fresh = visit(vis, dirty, a.dirty_cap, dcount, id, valid, lane);
-                    if (nb + 32 > kBuf) {
-                        n_dist += nb;
-                        const uint32_t r = flush<KIND, ORDER, CL>(a, m, nb, &sz, true, qv, lane);
-                        nk = min(nk, r);
-                        nb = 0;
-                    }
-                    const uint32_t bm = __ballot_sync(kFull, fresh);
-                    if (fresh) m.bi[nb + __popc(bm & lanemask_lt())] = id;
-                    nb += __popc(bm);
-                    __syncwarp();
                 }
             }
             __syncwarp();
         }
         if (nb) {
             n_dist += nb;
-            const uint32_t r = flush<KIND, ORDER, CL>(a, m, nb, &sz, true, qv, lane);
-            nk = min(nk, r);
+            nk = min(nk, flush<KIND, ORDER, CL>(a, m, nb, &sz, true, qv, lane));
             nb = 0;
         }
         k = nk <= last_k ? nk : last_k + 1;
     }
 
-    // Results and counters.
-    for (uint32_t i = lane; i < a.K; i += 32) a.out_ids[(size_t) q * a.K + i] = m.qi[i] & kIdMask;
+    // Results (original ids) and counters.
+    for (uint32_t i = lane; i < a.K; i += 32)
+        a.out_ids[(size_t) q * a.K + i] = __ldg(a.orig + (m.qi[i] & kIdMask));
     if (lane == 0 && a.out_stats) a.out_stats[q] = make_uint4(n_dist, n_expand, n_edges, n_iter);
     // Clear the visited words this query set.
     if (dcount <= a.dirty_cap) {
@@ -526,7 +621,7 @@ __device__ void search_one(const SearchArgs &a, const WarpMem &m, uint32_t q, ui
 }
 
 template <int KIND, int ORDER, int CL>
-__global__ void __launch_bounds__(256) search_kernel(SearchArgs a) {
+__global__ void __launch_bounds__(128, 6) search_kernel(SearchArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
     const int lane = threadIdx.x & 31;
     const int wid = threadIdx.x >> 5;
