@@ -160,6 +160,24 @@ int panns_search_device(panns_index *h, const panns_search_params *p, const floa
                         uint32_t nq, const uint32_t *init_ids, uint32_t *d_out_ids, void *stream,
                         panns_stats *stats);
 
+/* The batched search without any memory allocation, for callers that cannot
+ * allocate GPU memory once they are running (a serving process whose memory
+ * is all reserved by a framework's pool, a latency-bound loop, a plug-in in a
+ * host that forbids allocations after start-up). No counterpart in the
+ * reference, which allocates its scratch (set_L, is_visited) in the caller.
+ * d_queries: nq x d float32 and d_out_ids: nq x K u32 (original ids), both
+ * device pointers owned by the caller; `stream` is a cudaStream_t (NULL = the
+ * handle's stream). Modes NSG_SEQ, TOP_M and PSS_V5 with T = 1 (the PANNS init
+ * list), L <= 1024. All scratch comes from one fixed 32 MiB array in the
+ * library's device image: N, nq and the warp count must fit it, otherwise
+ * PANNS_EINVAL says so. The index must already be laid out on the GPU (one
+ * panns_search or panns_search_host call before). The first call on a device
+ * looks up the array's address; make it before any stream capture. Calls
+ * share the array: calls that overlap on the GPU race. Returns after the
+ * search has finished. */
+int panns_search_static(panns_index *h, const panns_search_params *p, const float *d_queries,
+                        uint32_t nq, uint32_t *d_out_ids, void *stream);
+
 /* Recall@k (k in {1, 5, 10, 20, 50, 100}) of result ids against a true-NN
  * list, with the reference's definition (PSS.cpp:191-230): a true top-k id
  * counts if it appears in result[0 : min(L, 100, k)]. true_ids: nq x true_k. */

@@ -875,3 +875,182 @@ int panns_load_true_nn(const char *path, uint32_t *nq, uint32_t *K, uint32_t *id
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// panns_search_static: the batched search without any memory allocation.
+//
+// Some callers cannot allocate GPU memory at search time: a server that
+// reserves all device memory for a framework's own pool at start-up, a
+// real-time loop where an allocation (and the device-wide synchronisation a
+// cudaFree implies) would break its latency budget, or a plug-in loaded into
+// a host process that forbids allocations after initialisation. For them this
+// entry point takes its scratch — the per-warp visited bitsets and cleared-word
+// lists, the work counter, the error word, the chain-major copy of the
+// queries and the init ids — from one fixed array of kStaticScratchBytes that
+// lives in the library's device image. Every GPU that loads the library holds
+// that array until the process exits.
+//
+// The first call on a device looks up the array's device address
+// (cudaGetSymbolAddress); make that first call before any stream capture.
+// All calls share the array and it keeps the last call's contents: each call
+// zeroes what must start at zero. Calls that overlap on the GPU (from two
+// threads, or on two streams) race on the array and must not be made.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+namespace {
+
+constexpr size_t kStaticScratchBytes = 32ull << 20;   // 32 MiB
+constexpr uint32_t kStaticMaxL = 1024;               // init ids held in the array
+constexpr uint32_t kStaticDirtyCap = 2048;           // cleared-word list per warp
+constexpr size_t kStaticHeader = 256;                // counter, error
+
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+std::mutex g_static_mu;
+void *g_static_addr[64] = {nullptr};
+
+int static_scratch_address(int device, unsigned char **out) {
+    if (device < 0 || device >= 64) return fail(PANNS_EINVAL, "panns_search_static: device index >= 64");
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    if (!g_static_addr[device]) {
+        void *ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_static_scratch);
+        if (e != cudaSuccess || !ptr)
+            return fail(PANNS_ECUDA, std::string("panns_search_static: cudaGetSymbolAddress: ") +
+                                         cudaGetErrorString(e));
+        g_static_addr[device] = ptr;
+    }
+    *out = static_cast<unsigned char *>(g_static_addr[device]);
+    return PANNS_OK;
+}
+
+}  // namespace
+
+extern "C" int panns_search_static(panns_index *h, const panns_search_params *p, const float *d_queries,
+                                   uint32_t nq, uint32_t *d_out_ids, void *stream) {
+    if (!h || !p) return fail(PANNS_EINVAL, "panns_search_static: NULL argument");
+    if (!h->ready)
+        return fail(PANNS_ESTATE, "panns_search_static: the index is not laid out on the GPU yet; "
+                                  "run one panns_search or panns_search_host first");
+    if (p->mode != PANNS_MODE_NSG_SEQ && p->mode != PANNS_MODE_TOP_M &&
+        !(p->mode == PANNS_MODE_PSS_V5 && p->T == 1))
+        return fail(PANNS_EINVAL, "panns_search_static: only NSG_SEQ, TOP_M and PSS_V5 with T = 1");
+    if (p->distance > PANNS_DIST_L2) return fail(PANNS_EINVAL, "panns_search_static: unknown distance");
+    if (p->L == 0 || p->L > h->n) return fail(PANNS_EINVAL, "panns_search_static: need 0 < L <= N");
+    if (p->K == 0 || p->K > p->L) return fail(PANNS_EINVAL, "panns_search_static: need 0 < K <= L");
+    if (p->L > kStaticMaxL)
+        return fail(PANNS_EINVAL, "panns_search_static: L = " + std::to_string(p->L) +
+                                      " exceeds the fixed scratch limit of " + std::to_string(kStaticMaxL));
+    if (p->mode == PANNS_MODE_TOP_M && (p->M == 0 || p->M > (uint32_t) kMaxM))
+        return fail(PANNS_EINVAL, "panns_search_static: TOP_M needs 1 <= M <= 64");
+    if (p->warps_per_block > 8 || p->flags) return fail(PANNS_EINVAL, "panns_search_static: bad params");
+    if (nq == 0) return PANNS_OK;
+    if (!d_queries || !d_out_ids) return fail(PANNS_EINVAL, "panns_search_static: NULL device buffer");
+    cudaStream_t st = stream ? (cudaStream_t) stream : h->stream;
+    CU(cudaSetDevice(h->device));
+    unsigned char *base = nullptr;
+    int rc = static_scratch_address(h->device, &base);
+    if (rc) return rc;
+
+    // Carve the fixed array: header | init ids | chain-major queries | cleared-word lists | bitsets.
+    const uint32_t vis_words = (h->n + 31) / 32;
+    const size_t off_init = kStaticHeader;
+    const size_t off_q = off_init + (size_t) kStaticMaxL * 4;
+    const size_t q_bytes = ((size_t) nq * h->dpad * 4 + 255) & ~(size_t) 255;
+    const size_t off_slots = off_q + q_bytes;
+    const size_t per_slot = (size_t) kStaticDirtyCap * 4 + (size_t) vis_words * 4;
+    if (off_slots + per_slot > kStaticScratchBytes)
+        return fail(PANNS_EINVAL, "panns_search_static: N = " + std::to_string(h->n) + " with nq = " +
+                                      std::to_string(nq) + " does not fit the fixed " +
+                                      std::to_string(kStaticScratchBytes >> 20) + " MiB scratch");
+    const uint32_t fit_slots = (uint32_t) ((kStaticScratchBytes - off_slots) / per_slot);
+
+    const int CL = (int) (h->dpad / 32);
+    const uint32_t kind = p->distance == PANNS_DIST_L2 ? KIND_L2 : KIND_IP;
+    const void *kern = kernel_for(kind, ORDER_PANNS, CL);
+    if (!kern) return fail(PANNS_EINVAL, "panns_search_static: unsupported dimension");
+    const uint32_t M = p->mode == PANNS_MODE_TOP_M ? p->M : 1u;
+    const uint32_t qcap = ((p->L + 31) / 32) * 32;
+    const uint32_t wpb = p->warps_per_block ? p->warps_per_block : 4u;
+    const size_t smem = (size_t) wpb * warp_smem_bytes(qcap);
+    CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+    int per_sm = 0;
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (int) wpb * 32, smem));
+    if (per_sm < 1) return fail(PANNS_EINVAL, "panns_search_static: L too large for shared memory");
+    uint32_t blocks = std::min((uint32_t) per_sm * (uint32_t) h->num_sms, (nq + wpb - 1) / wpb);
+    blocks = std::min(blocks, fit_slots / wpb);
+    if (blocks == 0)
+        return fail(PANNS_EINVAL, "panns_search_static: N = " + std::to_string(h->n) +
+                                      " leaves room for fewer than one block of warps in the fixed scratch");
+    const uint32_t slots = blocks * wpb;
+
+    // Init ids (the PANNS list: entry's neighbours deduplicated, then entry+1,
+    // entry+2, ...), as device ids, built in a stack buffer.
+    uint32_t init[kStaticMaxL];
+    uint32_t end = 0;
+    const uint64_t e0 = h->off[h->entry], e1 = h->off[h->entry + 1];
+    for (uint64_t e = e0; e < e1 && end < p->L; ++e) {
+        const uint32_t v = h->nbrs[e];
+        bool dup = false;
+        for (uint32_t i = 0; i < end && !dup; ++i) dup = init[i] == v;
+        if (!dup) init[end++] = v;
+    }
+    const uint32_t from_nbrs = end;
+    for (uint32_t t = h->entry + 1; end < p->L; ++t) {
+        if (t == h->n) t = 0;
+        bool dup = false;
+        for (uint32_t i = 0; i < from_nbrs && !dup; ++i) dup = init[i] == t;
+        if (!dup) init[end++] = t;
+    }
+    for (uint32_t i = 0; i < end; ++i) init[i] = h->inv[init[i]];
+
+    uint32_t *counter = reinterpret_cast<uint32_t *>(base);
+    uint32_t *err_word = counter + 1;
+    uint32_t *d_init = reinterpret_cast<uint32_t *>(base + off_init);
+    float *d_qcm = reinterpret_cast<float *>(base + off_q);
+    uint32_t *d_dirty = reinterpret_cast<uint32_t *>(base + off_slots);
+    uint32_t *d_vis = d_dirty + (size_t) slots * kStaticDirtyCap;
+    CU(cudaMemsetAsync(base, 0, kStaticHeader, st));
+    CU(cudaMemsetAsync(d_vis, 0, (size_t) slots * vis_words * 4, st));
+    CU(cudaMemcpyAsync(d_init, init, (size_t) end * 4, cudaMemcpyHostToDevice, st));
+    {
+        const uint64_t total = (uint64_t) nq * h->dpad;
+        const int pb = (int) std::min<uint64_t>((total + 255) / 256, (uint64_t) h->num_sms * 32);
+        permute_rows_kernel<<<std::max(pb, 1), 256, 0, st>>>(d_queries, d_qcm, nq, (int) h->d,
+                                                             (int) h->dpad, nullptr);
+        CU(cudaGetLastError());
+    }
+    SearchArgs a;
+    a.vec = reinterpret_cast<const float4 *>(h->vec.p);
+    a.norms = h->norms.p;
+    a.head = h->head.p;
+    a.ovf_off = h->ovf_off.p;
+    a.ovf = h->ovf.p;
+    a.orig = h->orig.p;
+    a.n = h->n;
+    a.queries = reinterpret_cast<const float4 *>(d_qcm);
+    a.nq = nq;
+    a.init_ids = d_init;
+    a.init_stride = 0;
+    a.K = p->K;
+    a.L = p->L;
+    a.M = M;
+    a.out_ids = d_out_ids;
+    a.out_stats = nullptr;
+    a.visited = d_vis;
+    a.vis_words = vis_words;
+    a.dirty = d_dirty;
+    a.dirty_cap = kStaticDirtyCap;
+    a.counter = counter;
+    a.error = err_word;
+    a.queue_cap = qcap;
+    void *args[] = {&a};
+    CU(cudaLaunchKernel(kern, dim3(blocks), dim3(wpb * 32), args, smem, st));
+    uint32_t err = 0;
+    CU(cudaMemcpyAsync(&err, err_word, 4, cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    if (err & ERR_BAD_ID) return fail(PANNS_EDEVICE, "panns_search_static: a neighbour id >= N");
+    if (err & ERR_BAD_INIT) return fail(PANNS_EDEVICE, "panns_search_static: init id >= N");
+    return PANNS_OK;
+}
