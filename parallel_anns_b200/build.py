@@ -14,9 +14,9 @@ import sys
 PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 SO = os.path.join(PKG, "libpanns_b200.so")
-SOURCES = [os.path.join(PKG, "csrc", "panns_abi.cu")]
-DEPS = SOURCES + [
-    os.path.join(PKG, "csrc", "search_kernel.cuh"),
+SOURCES = [os.path.join(PKG, "csrc", f) for f in ("panns_abi.cu", "search_kernels.cu", "pss_kernels.cu")]
+DEPS = SOURCES + [os.path.join(PKG, "csrc", f) for f in
+                  ("search_kernel.cuh", "pss_kernel.cuh", "kernels.h")] + [
     os.path.join(ROOT, "include", "panns_b200.h"),
 ]
 
@@ -24,7 +24,6 @@ NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
     "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
-    "-shared",
 ]
 
 
@@ -43,12 +42,26 @@ def up_to_date() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False, extra=None) -> str:
+    """Compile every source to an object in parallel, then link the shared library."""
     if not force and up_to_date():
         return SO
-    cmd = [nvcc()] + NVCC_FLAGS + (extra or []) + ["-o", SO + ".tmp"] + SOURCES + ["-lcudart"]
-    if verbose:
-        print(" ".join(cmd), file=sys.stderr)
-    subprocess.run(cmd, check=True, cwd=PKG)
+    objdir = os.path.join(PKG, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    procs = []
+    objs = []
+    for src in SOURCES:
+        obj = os.path.join(objdir, os.path.basename(src) + ".o")
+        objs.append(obj)
+        cmd = [nvcc()] + NVCC_FLAGS + (extra or []) + ["-c", src, "-o", obj]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        procs.append((cmd, subprocess.Popen(cmd, cwd=PKG)))
+    for cmd, p in procs:
+        if p.wait() != 0:
+            raise subprocess.CalledProcessError(p.returncode, cmd)
+    link = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", SO + ".tmp"] + objs + [
+        "-lcudart"]
+    subprocess.run(link, check=True, cwd=PKG)
     os.replace(SO + ".tmp", SO)
     return SO
 

@@ -1,0 +1,23 @@
+// Kernel entry points compiled in their own translation units
+// (search_kernels.cu, pss_kernels.cu), looked up by the host launch code.
+#pragma once
+#include <stdint.h>
+
+namespace panns {
+
+// Chain blocks (float4 x 8 = 32 floats) per padded row for dimension d: the
+// smallest instantiated value >= ceil(d / 32); rows are zero-padded to it.
+inline uint32_t chain_blocks(uint32_t d) {
+    const uint32_t need = (d + 31) / 32;
+    static const uint32_t avail[] = {1, 2, 3, 4, 6, 8};
+    for (uint32_t a : avail)
+        if (a >= need) return a;
+    return 0;
+}
+
+// search_kernel<KIND, ORDER, CL> (search_kernel.cuh); nullptr if not built.
+const void *search_kernel_ptr(uint32_t kind, uint32_t order, int CL);
+// pss_kernel<KIND, CL> (pss_kernel.cuh); nullptr if not built.
+const void *pss_kernel_ptr(uint32_t kind, int CL);
+
+}  // namespace panns

@@ -13,6 +13,8 @@
 
 #include "../../include/panns_b200.h"
 #include "search_kernel.cuh"
+#include "pss_kernel.cuh"
+#include "kernels.h"
 
 using namespace panns;
 
@@ -213,7 +215,7 @@ int panns_close(panns_index *h) {
 
 static int upload_chain_major(panns_index *h, const float *rows, uint64_t count, uint32_t d,
                               DevBuf<float> &dst) {
-    const uint32_t dpad = ((d + 31) / 32) * 32;
+    const uint32_t dpad = 32u * chain_blocks(d);
     CU(h->raw.ensure(count * d));
     CU(dst.ensure(count * dpad));
     CU(cudaMemcpyAsync(h->raw.p, rows, count * d * sizeof(float), cudaMemcpyHostToDevice, h->stream));
@@ -244,7 +246,7 @@ int panns_set_base(panns_index *h, const float *data, uint32_t n, uint32_t d, ui
     CU(cudaStreamSynchronize(h->stream));
     h->n = n;
     h->d = d;
-    h->dpad = ((d + 31) / 32) * 32;
+    h->dpad = 32u * chain_blocks(d);
     h->storage = storage;
     h->ready = false;
     return PANNS_OK;
@@ -556,29 +558,6 @@ int panns_efanna_init_ids(const panns_index *h, uint32_t L, uint32_t nq, int32_t
 // ---------------------------------------------------------------------------
 namespace {
 
-template <int KIND, int ORDER>
-const void *pick_kernel(int CL) {
-    switch (CL) {
-        case 1: return (const void *) search_kernel<KIND, ORDER, 1>;
-        case 2: return (const void *) search_kernel<KIND, ORDER, 2>;
-        case 3: return (const void *) search_kernel<KIND, ORDER, 3>;
-        case 4: return (const void *) search_kernel<KIND, ORDER, 4>;
-        case 5: return (const void *) search_kernel<KIND, ORDER, 5>;
-        case 6: return (const void *) search_kernel<KIND, ORDER, 6>;
-        case 7: return (const void *) search_kernel<KIND, ORDER, 7>;
-        case 8: return (const void *) search_kernel<KIND, ORDER, 8>;
-    }
-    return nullptr;
-}
-
-const void *kernel_for(uint32_t kind, uint32_t order, int CL) {
-    if (kind == KIND_IP)
-        return order == ORDER_PANNS ? pick_kernel<KIND_IP, ORDER_PANNS>(CL)
-                                    : pick_kernel<KIND_IP, ORDER_EFANNA>(CL);
-    return order == ORDER_PANNS ? pick_kernel<KIND_L2, ORDER_PANNS>(CL)
-                                : pick_kernel<KIND_L2, ORDER_EFANNA>(CL);
-}
-
 int check_params(panns_index *h, const panns_search_params *p) {
     if (!p) return fail(PANNS_EINVAL, "search: NULL params");
     int rc = finalize(h);
@@ -592,7 +571,9 @@ int check_params(panns_index *h, const panns_search_params *p) {
         return fail(PANNS_EINVAL, "search: TOP_M needs 1 <= M <= 64");
     if (p->mode == PANNS_MODE_PSS_V5) {
         if (p->T == 0 || p->X == 0) return fail(PANNS_EINVAL, "search: PSS_V5 needs T >= 1 and X >= 1");
-        if (p->T > 1) return fail(PANNS_EINVAL, "search: PSS_V5 with T > 1 is not available in this build");
+        if (p->T > 64) return fail(PANNS_EINVAL, "search: PSS_V5 needs T <= 64");
+        const uint32_t Ll = p->L_local ? p->L_local : p->L;
+        if (Ll > 8192) return fail(PANNS_EINVAL, "search: L_local > 8192 is not supported");
     }
     if (p->warps_per_block > 8) return fail(PANNS_EINVAL, "search: warps_per_block must be <= 8");
     if (p->flags) return fail(PANNS_EINVAL, "search: flags must be 0");
@@ -609,12 +590,21 @@ static int launch_search(panns_index *h, const panns_search_params *p, const flo
     const int CL = (int) (h->dpad / 32);
     const uint32_t order = p->mode == PANNS_MODE_EFANNA ? ORDER_EFANNA : ORDER_PANNS;
     const uint32_t kind = p->distance == PANNS_DIST_L2 ? KIND_L2 : KIND_IP;
-    const void *kern = kernel_for(kind, order, CL);
+    const bool pss = p->mode == PANNS_MODE_PSS_V5 && p->T > 1;
+    const void *kern = pss ? pss_kernel_ptr(kind, CL) : search_kernel_ptr(kind, order, CL);
     if (!kern) return fail(PANNS_EINVAL, "search: unsupported dimension");
     const uint32_t M = p->mode == PANNS_MODE_TOP_M ? p->M : 1u;
     const uint32_t qcap = ((p->L + 31) / 32) * 32;
-    const uint32_t wpb = p->warps_per_block ? p->warps_per_block : 4u;
-    const size_t smem = (size_t) wpb * warp_smem_bytes(qcap);
+    const uint32_t L_local = p->L_local ? p->L_local : p->L;
+    const uint32_t wcap = ((L_local + 31) / 32) * 32;
+    uint32_t wpb = p->warps_per_block ? p->warps_per_block : 4u;
+    size_t per_warp = pss ? pss_smem_bytes(qcap, p->T, wcap) : warp_smem_bytes(qcap);
+    if (pss && !p->warps_per_block) {
+        while (wpb > 1 && wpb * per_warp > (100u << 10)) --wpb;
+    }
+    if (per_warp > (227u << 10))
+        return fail(PANNS_EINVAL, "search: the queues (L, T x L_local) do not fit in shared memory");
+    const size_t smem = (size_t) wpb * per_warp;
     CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
     int per_sm = 0;
     CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (int) wpb * 32, smem));
@@ -668,9 +658,16 @@ static int launch_search(panns_index *h, const panns_search_params *p, const flo
     a.counter = h->counter.p;
     a.error = h->error.p;
     a.queue_cap = qcap;
+    PssArgs pa;
+    pa.s = a;
+    pa.T = p->T;
+    pa.L_local = L_local;
+    pa.X = p->X;
+    pa.wcap = wcap;
     void *args[] = {&a};
+    void *pargs[] = {&pa};
     if (time_it) CU(cudaEventRecord(h->ev0, stream));
-    CU(cudaLaunchKernel(kern, dim3(blocks), dim3(wpb * 32), args, smem, stream));
+    CU(cudaLaunchKernel(kern, dim3(blocks), dim3(wpb * 32), pss ? pargs : args, smem, stream));
     if (time_it) CU(cudaEventRecord(h->ev1, stream));
     return PANNS_OK;
 }
@@ -968,7 +965,7 @@ extern "C" int panns_search_static(panns_index *h, const panns_search_params *p,
 
     const int CL = (int) (h->dpad / 32);
     const uint32_t kind = p->distance == PANNS_DIST_L2 ? KIND_L2 : KIND_IP;
-    const void *kern = kernel_for(kind, ORDER_PANNS, CL);
+    const void *kern = search_kernel_ptr(kind, ORDER_PANNS, CL);
     if (!kern) return fail(PANNS_EINVAL, "panns_search_static: unsupported dimension");
     const uint32_t M = p->mode == PANNS_MODE_TOP_M ? p->M : 1u;
     const uint32_t qcap = ((p->L + 31) / 32) * 32;

@@ -108,7 +108,7 @@ struct WarpMem {
     uint32_t *pre;
 };
 
-__device__ __forceinline__ WarpMem carve(uint8_t *base, uint32_t queue_cap) {
+static __device__ __forceinline__ WarpMem carve(uint8_t *base, uint32_t queue_cap) {
     WarpMem m;
     m.qd = reinterpret_cast<float *>(base);
     m.qi = reinterpret_cast<uint32_t *>(m.qd + queue_cap);
@@ -121,7 +121,7 @@ __device__ __forceinline__ WarpMem carve(uint8_t *base, uint32_t queue_cap) {
     return m;
 }
 
-__device__ __forceinline__ uint32_t lanemask_lt() {
+static __device__ __forceinline__ uint32_t lanemask_lt() {
     uint32_t m;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
     return m;
@@ -154,7 +154,7 @@ __device__ __forceinline__ float chain(const float4 (&x)[CL], const float4 (&qv)
     return acc;
 }
 
-__device__ __forceinline__ float lane_sum8(float acc, int lane) {
+static __device__ __forceinline__ float lane_sum8(float acc, int lane) {
     const int base = lane & ~7;
     float s = __shfl_sync(kFull, acc, base);
 #pragma unroll
@@ -225,7 +225,8 @@ __device__ __forceinline__ uint32_t queue_rank(const float *qd, const uint32_t *
     return lo;
 }
 
-// Number of sorted fresh elements that precede a queue element (d, id).
+// Number of sorted fresh elements that precede a queue element (d, id). Fresh
+// ids may carry the checked bit (worker queues merged into the master).
 template <int ORDER>
 __device__ __forceinline__ uint32_t fresh_rank(const float *bd, const uint32_t *bi, uint32_t cnt,
                                                float d, uint32_t id, const uint32_t *orig) {
@@ -235,7 +236,7 @@ __device__ __forceinline__ uint32_t fresh_rank(const float *bd, const uint32_t *
         const float md = bd[mid];
         bool before;
         if (ORDER == ORDER_PANNS) {
-            before = md < d || (md == d && __ldg(orig + bi[mid]) < __ldg(orig + id));
+            before = md < d || (md == d && __ldg(orig + (bi[mid] & kIdMask)) < __ldg(orig + id));
         } else {
             before = md < d;
         }
@@ -314,58 +315,65 @@ __device__ void warp_sort(float *bd, uint32_t *bi, uint32_t *bk, uint32_t cnt,
     }
 }
 
-// Merge the sorted fresh elements (bd, bi)[0..cnt) into the queue of size *sz
-// (capacity L). Returns the position of the first fresh element if it was
-// inserted (< L), else L. Uses bk as scratch.
+// Merge the sorted fresh elements (bd, bi)[0..cnt) into the queue (qd, qi)
+// of size *sz and capacity cap. Returns the position of the first fresh
+// element if it was inserted (< cap), else cap. Uses bk as scratch.
 template <int ORDER>
-__device__ uint32_t warp_merge(const WarpMem &m, uint32_t *sz, uint32_t L, uint32_t cnt,
-                               const uint32_t *orig, int lane) {
+__device__ uint32_t merge_into(float *qd, uint32_t *qi, uint32_t *sz, uint32_t cap, const float *bd,
+                               const uint32_t *bi, uint32_t *bk, uint32_t cnt, const uint32_t *orig,
+                               int lane) {
     const uint32_t qsz = *sz;
-    if (cnt == 0) return L;
+    if (cnt == 0) return cap;
     // Merged position of each fresh element: its index plus its rank in the old queue.
     for (uint32_t i = lane; i < cnt; i += 32)
-        m.bk[i] = i + queue_rank<ORDER>(m.qd, m.qi, qsz, m.bd[i], m.bi[i], orig);
+        bk[i] = i + queue_rank<ORDER>(qd, qi, qsz, bd[i], bi[i] & kIdMask, orig);
     __syncwarp();
-    const uint32_t p0 = m.bk[0];
-    if (p0 >= L) return L;
+    const uint32_t p0 = bk[0];
+    if (p0 >= cap) return cap;
     // Move queue elements [p0, qsz) to their merged positions, top chunk first;
     // a chunk is read completely before any of it is written.
     for (int32_t top = (int32_t) qsz - 1; top >= (int32_t) p0; top -= 32) {
         const int32_t j = top - lane;
         float d = 0.f;
-        uint32_t id = 0, np = L;
+        uint32_t id = 0, np = cap;
         if (j >= (int32_t) p0) {
-            d = m.qd[j];
-            id = m.qi[j];
-            np = (uint32_t) j + fresh_rank<ORDER>(m.bd, m.bi, cnt, d, id & kIdMask, orig);
+            d = qd[j];
+            id = qi[j];
+            np = (uint32_t) j + fresh_rank<ORDER>(bd, bi, cnt, d, id & kIdMask, orig);
         }
         __syncwarp();
-        if (np < L) {
-            m.qd[np] = d;
-            m.qi[np] = id;
+        if (np < cap) {
+            qd[np] = d;
+            qi[np] = id;
         }
         __syncwarp();
     }
     for (uint32_t i = lane; i < cnt; i += 32) {
-        const uint32_t np = m.bk[i];
-        if (np < L) {
-            m.qd[np] = m.bd[i];
-            m.qi[np] = m.bi[i];
+        const uint32_t np = bk[i];
+        if (np < cap) {
+            qd[np] = bd[i];
+            qi[np] = bi[i];
         }
     }
     __syncwarp();
-    *sz = min(L, qsz + cnt);
+    *sz = min(cap, qsz + cnt);
     return p0;
 }
 
+template <int ORDER>
+__device__ __forceinline__ uint32_t warp_merge(const WarpMem &m, uint32_t *sz, uint32_t L, uint32_t cnt,
+                                               const uint32_t *orig, int lane) {
+    return merge_into<ORDER>(m.qd, m.qi, sz, L, m.bd, m.bi, m.bk, cnt, orig, lane);
+}
+
 // Visited bitset: test-and-set returns the previous word.
-__device__ __forceinline__ uint32_t visit_issue(uint32_t *vis, uint32_t id, bool valid) {
+static __device__ __forceinline__ uint32_t visit_issue(uint32_t *vis, uint32_t id, bool valid) {
     return valid ? atomicOr(vis + (id >> 5), 1u << (id & 31)) : kFull;
 }
 
 // Record the words that went from zero to non-zero (only those are cleared
 // after the query).
-__device__ __forceinline__ void note_dirty(uint32_t *dirty, uint32_t dirty_cap, uint32_t &dcount,
+static __device__ __forceinline__ void note_dirty(uint32_t *dirty, uint32_t dirty_cap, uint32_t &dcount,
                                            bool first, uint32_t word) {
     const uint32_t bm = __ballot_sync(kFull, first);
     if (first) {

@@ -177,3 +177,20 @@ def test_gpu_errors(mix20k, N):
     ref, _ = O.search_top_m(base, O.Graph.from_nsg(g), q[:5], 10, 20, 1)
     assert np.array_equal(a, ref)
     ix.close()
+
+
+@pytest.mark.parametrize("T,X,Ll", [(2, 1, 0), (4, 2, 0), (8, 4, 0), (3, 1, 64), (16, 8, 0), (5, 3, 300)])
+def test_gpu_pss_workers_match_oracle(mix20k, N, T, X, Ll):
+    """PSS_v5 with T queues: the GPU runs the oracle's fixed round-robin
+    schedule, so ids and distance counts match exactly."""
+    base, q, g = mix20k
+    G = O.Graph.from_nsg(g)
+    ix = gpu_index(base, g, q)
+    L = 200
+    for dist, kind in ((N.DIST_NORM_IP, O.DIST_IP_NORM), (N.DIST_L2, O.DIST_L2)):
+        ids, st = ix.search(K=100, L=L, mode=N.MODE_PSS_V5, distance=dist, T=T, X=X, L_local=Ll)
+        ref, nd = O.search_pss(base, G, q, 100, L, Ll or L, X, T, kind=kind)
+        bad = np.nonzero((ids != ref).any(1))[0]
+        assert bad.size == 0, f"T={T} X={X} Ll={Ll} dist={dist}: rows {bad[:8].tolist()}"
+        assert st["n_dist"] == nd
+    ix.close()
