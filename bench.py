@@ -181,86 +181,120 @@ def bench_ours(args):
     gts = gt_all[rank * args.nq:(rank + 1) * args.nq]
     nq, d, K = qs.shape[0], qs.shape[1], 100
 
-    ix = Index(local)
-    ix.set_base(W["base"])
-    ix.set_graph(W["graph"])
-    ix.set_queries(qs)
+    # One handle with the BF16 copy (its float32 rows serve the exact search),
+    # one with the FP8 copy.
+    handles = {}
+    for store in (N.STORE_BF16, N.STORE_FP8):
+        ix = Index(local)
+        ix.set_base(W["base"], storage=store)
+        ix.set_graph(W["graph"])
+        ix.set_queries(qs)
+        handles[store] = ix
+    handles[N.STORE_FP32] = handles[N.STORE_BF16]
+    names = {N.STORE_FP32: "fp32", N.STORE_BF16: "bf16", N.STORE_FP8: "fp8"}
 
-    def run(L, M):
+    def run(L, M, store):
         mode = N.MODE_NSG_SEQ if M == 1 else N.MODE_TOP_M
-        return ix.search(K=K, L=L, mode=mode, distance=N.DIST_NORM_IP, M=M)
+        return handles[store].search(K=K, L=L, mode=mode, distance=N.DIST_NORM_IP, M=M, storage=store)
 
-    # Operating point: per M the smallest swept L reaching the recall target;
-    # the fastest of those. Decided on rank 0, shared with every rank.
+    # Operating points: per (storage, M) the smallest swept L reaching the
+    # recall target; per storage the fastest of those. Decided on rank 0.
     sweep = []
-    if args.L and args.M:
-        choice = (args.L, args.M)
-    else:
-        best = None
+    best = {}
+    stores = [args.storage] if args.storage is not None else [N.STORE_FP32, N.STORE_BF16, N.STORE_FP8]
+    for store in stores:
         for M in ([args.M] if args.M else M_SWEEP):
             for L in ([args.L] if args.L else L_SWEEP):
-                ids, st = run(L, M)
-                ids, st = run(L, M)
+                run(L, M, store)
+                ids, st = run(L, M, store)
                 rec = recall(ids, gts, L, 100)
-                sweep.append({"M": M, "L": L, "recall100": round(rec, 5),
+                sweep.append({"storage": names[store], "M": M, "L": L, "recall100": round(rec, 5),
                               "qps": round(nq / (st["kernel_ms"] / 1e3), 1)})
-                if rec >= RECALL_TARGET:
-                    if best is None or st["kernel_ms"] < best[0]:
-                        best = (st["kernel_ms"], L, M)
+                if rec >= RECALL_TARGET or (args.L and args.M):
+                    if store not in best or st["kernel_ms"] < best[store][0]:
+                        best[store] = (st["kernel_ms"], L, M)
                     break
-        if best is None:
-            best = (0, L_SWEEP[-1], 1)
-        choice = (best[1], best[2])
+    for store in stores:
+        best.setdefault(store, (1e30, L_SWEEP[-1], 1))
+    head_store = min(best, key=lambda k: best[k][0])
+    choice = [head_store, best[head_store][1], best[head_store][2]]
+    plain = [N.STORE_FP32, best.get(N.STORE_FP32, best[head_store])[1],
+             best.get(N.STORE_FP32, best[head_store])[2]]
     if world > 1:
-        t = torch.tensor(list(choice), dtype=torch.int64, device="cuda")
+        t = torch.tensor(choice + plain, dtype=torch.int64, device="cuda")
         dist.broadcast(t, 0)
-        choice = (int(t[0]), int(t[1]))
-    L, M = choice
+        choice, plain = [int(x) for x in t[:3]], [int(x) for x in t[3:]]
+    store, L, M = choice
     if rank == 0:
-        log(f"operating point L={L} M={M}; sweep {sweep}")
+        log(f"operating point storage={names[store]} L={L} M={M}; plain fp32 L={plain[1]} M={plain[2]}; "
+            f"sweep {sweep}")
 
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
     sampler = ClockSampler(local)
-    for _ in range(args.warmup):
-        run(L, M)
-    sampler.start()
-    barrier()
-    torch.cuda.synchronize()
-    kernel_ms = 0.0
-    tot = {"n_dist": 0, "n_edges": 0, "n_expand": 0, "n_iter": 0}
-    last_ids = None
-    for _ in range(args.steps):
-        flush.zero_()
+
+    def timed(cfg):
+        st_, L_, M_ = cfg
+        for _ in range(args.warmup):
+            run(L_, M_, st_)
+        barrier()
         torch.cuda.synchronize()
-        last_ids, st = run(L, M)
-        kernel_ms += st["kernel_ms"]
-        for k in tot:
-            tot[k] += st[k]
-    barrier()
-    torch.cuda.synchronize()
+        kms = 0.0
+        tot_ = {"n_dist": 0, "n_edges": 0, "n_expand": 0, "n_iter": 0}
+        ids_ = None
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            ids_, st = run(L_, M_, st_)
+            kms += st["kernel_ms"]
+            for k in tot_:
+                tot_[k] += st[k]
+        barrier()
+        torch.cuda.synchronize()
+        return kms, tot_, ids_
+
+    sampler.start()
+    kernel_ms, tot, last_ids = timed(choice)
     kernel_ms_max = max_over_ranks(kernel_ms)
     rec = recall(last_ids, gts, L, 100)
+    if (plain[1], plain[2]) == (L, M) and store == N.STORE_FP32:
+        p_ms, p_ids = kernel_ms, last_ids
+    else:
+        p_ms, _, p_ids = timed(plain)
+    p_ms_max = max_over_ranks(p_ms)
+    p_rec = recall(p_ids, gts, plain[1], 100)
 
     # End to end through the host-pointer C ABI call.
     mode = N.MODE_NSG_SEQ if M == 1 else N.MODE_TOP_M
+    ixh = handles[store]
     for _ in range(args.warmup):
-        ix.search(qs, K=K, L=L, mode=mode, M=M)
+        ixh.search(qs, K=K, L=L, mode=mode, M=M, storage=store)
     barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(args.steps):
         flush.zero_()
         torch.cuda.synchronize()
-        ids_e2e, st_e2e = ix.search(qs, K=K, L=L, mode=mode, M=M)
+        ids_e2e, st_e2e = ixh.search(qs, K=K, L=L, mode=mode, M=M, storage=store)
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     clocks = sampler.stop()
     assert np.array_equal(ids_e2e, last_ids)
 
+    # Distance error of the returned ids against float64 (reduced storage re-ranks in float32).
+    ids64 = last_ids[: min(200, nq)].astype(np.int64)
+    qq = qs[: ids64.shape[0]].astype(np.float64)
+    d64 = ((W["base"][ids64].astype(np.float64) - qq[:, None, :]) ** 2).sum(-1)
+    g64 = ((W["base"][gts[: ids64.shape[0], :K].astype(np.int64)].astype(np.float64) - qq[:, None, :]) ** 2).sum(-1)
+    dist_err = float(np.mean(np.abs(np.sort(d64, 1) - np.sort(g64, 1)) / np.maximum(np.sort(g64, 1), 1e-12)))
+
     # Roofline of the search kernel: algorithmic bytes per launch
-    # = n_dist * (4d + 4 norm) + 4 * sum(1 + degree) over expansions + nq * (4d + 4K).
+    # = n_dist * (s*d + 4 norm) + 4 * sum(1 + degree) over expansions + nq * (4d + 4K)
+    #   (+ nq * L * (4d + 4) for the float32 re-rank of a reduced copy).
     steps = args.steps
-    alg_bytes = (tot["n_dist"] * (4 * d + 4) + 4 * tot["n_edges"]) / steps + nq * (4 * d + 4 * K)
+    s_el = {N.STORE_FP32: 4, N.STORE_BF16: 2, N.STORE_FP8: 1}[store]
+    alg_bytes = (tot["n_dist"] * (s_el * d + 4) + 4 * tot["n_edges"]) / steps + nq * (4 * d + 4 * K)
+    if store != N.STORE_FP32:
+        alg_bytes += nq * L * (4 * d + 4)
     launch_s = kernel_ms / steps / 1e3
     achieved = alg_bytes / launch_s / 1e9
     peak, peak_kind = measured_peak_hbm()
@@ -270,7 +304,7 @@ def bench_ours(args):
         try:
             with open(tp) as f:
                 tj = json.load(f)
-            if tj.get("L") == L and tj.get("M") == M and tj.get("n") == args.n:
+            if (tj.get("L"), tj.get("M"), tj.get("n"), tj.get("storage")) == (L, M, args.n, names[store]):
                 traffic = tj["dram_bytes_per_query"] * nq
         except Exception:
             traffic = None
@@ -290,12 +324,15 @@ def bench_ours(args):
             "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
             "steps": steps, "warmup": args.warmup,
             "ms_per_step": round(kernel_ms_max / steps, 4), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "batched FP32 search, 1M x 96d mixture64 (sigma 0.3, unit norm), "
+            "scaling": "weak", "vs_baseline": None, "dtype": names[store], "data": "synthetic",
+            "config": {"workload": "batched search, 1M x 96d mixture64 (sigma 0.3, unit norm), "
                                    "NSG-style graph R=50, 10k queries per GPU, K=100",
                        "n": args.n, "d": d, "queries_per_gpu": nq, "K": K, "L": L, "M": M,
+                       "storage": names[store], "accumulate": "f32",
+                       "rerank": "exact f32 of the final L" if store != N.STORE_FP32 else None,
                        "mode": "NSG_SEQ" if M == 1 else "TOP_M", "distance": "NORM_IP",
                        "recall100": round(rec, 5), "recall_target": RECALL_TARGET,
+                       "mean_rel_distance_error_vs_fp64": dist_err,
                        "avg_degree": round(W["meta"]["avg_degree"], 3), "width": W["meta"]["width"],
                        "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (384 MB base) and a 256 MB L2 flush before each step",
@@ -308,12 +345,16 @@ def bench_ours(args):
                     "h2d_bytes_per_step": nq * d * 4 + L * 4,
                     "d2h_bytes_per_step": nq * K * 4 + nq * 16},
             "gpu_launches": steps,
+            "plain_fp32": {"value": round(nq * world * steps / (p_ms_max / 1e3), 1), "unit": UNIT,
+                           "L": plain[1], "M": plain[2], "recall100": round(p_rec, 5),
+                           "ms_per_step": round(p_ms_max / steps, 4)},
             "counts_per_query": {k: round(v / steps / nq, 2) for k, v in tot.items()},
             "clocks": clocks,
             "cpu_baseline": cpu_base,
         }
         print(json.dumps(line), flush=True)
-    ix.close()
+    for ixx in set(handles.values()):
+        ixx.close()
     if world > 1:
         dist.destroy_process_group()
 
@@ -401,6 +442,8 @@ def main():
     ap.add_argument("--nq", type=int, default=10_000, help="queries per GPU")
     ap.add_argument("--L", type=int, default=0, help="fix L (default: recall-driven sweep)")
     ap.add_argument("--M", type=int, default=0, help="fix M (default: sweep)")
+    ap.add_argument("--storage", type=int, default=None, choices=[0, 1, 2],
+                    help="fix the storage (0 fp32, 1 bf16, 2 fp8; default: sweep)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -74,6 +74,9 @@ typedef struct {
     uint32_t L_local;     /* PSS_V5: worker queue capacity (0 = L) */
     uint32_t X;           /* PSS_V5: expansions per worker per stage (>= 1) */
     uint32_t warps_per_block; /* 0 = autotuned */
+    uint32_t storage;     /* panns_storage the search distances use: FP32 (exact), or
+                             the reduced copy built by panns_set_base (NSG_SEQ / TOP_M
+                             only; the final L are re-ranked in exact FP32) */
     uint32_t flags;       /* reserved, must be 0 */
 } panns_search_params;
 
@@ -103,7 +106,8 @@ int panns_close(panns_index *h);
 /* Base vectors, n x d float32 row-major (host pointer, copied).
  * Replaces Searching::load_data_load (PSS.cpp:14-28) with the file already
  * read; d must be a multiple of 8 (the reference's 8-lane kernels read
- * past the row otherwise). */
+ * past the row otherwise). `storage` BF16 or FP8 also builds that reduced
+ * copy (the float32 rows are always kept, for exact searches and re-ranks). */
 int panns_set_base(panns_index *h, const float *data, uint32_t n, uint32_t d, uint32_t storage);
 /* Read an fvecs file (include/utils.h:95-138 DiskIO::load_data) and call
  * panns_set_base. */

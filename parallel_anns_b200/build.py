@@ -14,9 +14,11 @@ import sys
 PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 SO = os.path.join(PKG, "libpanns_b200.so")
-SOURCES = [os.path.join(PKG, "csrc", f) for f in ("panns_abi.cu", "search_kernels.cu", "pss_kernels.cu")]
+SOURCES = [os.path.join(PKG, "csrc", f) for f in
+           ("panns_abi.cu", "search_kernels_fp32_ip.cu", "search_kernels_fp32_l2.cu",
+            "search_kernels_bf16.cu", "search_kernels_fp8.cu", "pss_kernels.cu")]
 DEPS = SOURCES + [os.path.join(PKG, "csrc", f) for f in
-                  ("search_kernel.cuh", "pss_kernel.cuh", "kernels.h")] + [
+                  ("search_kernel.cuh", "pss_kernel.cuh", "kernels.h", "search_kernels.inc")] + [
     os.path.join(ROOT, "include", "panns_b200.h"),
 ]
 

@@ -15,8 +15,18 @@ inline uint32_t chain_blocks(uint32_t d) {
     return 0;
 }
 
-// search_kernel<KIND, ORDER, CL> (search_kernel.cuh); nullptr if not built.
-const void *search_kernel_ptr(uint32_t kind, uint32_t order, int CL);
+// search_kernel<KIND, ORDER, CL, STORE> (search_kernel.cuh), one function per
+// translation unit; nullptr if that combination is not built.
+const void *search_kernel_ptr_fp32_ip(uint32_t kind, uint32_t order, int CL);
+const void *search_kernel_ptr_fp32_l2(uint32_t kind, uint32_t order, int CL);
+const void *search_kernel_ptr_bf16(uint32_t kind, uint32_t order, int CL);
+const void *search_kernel_ptr_fp8(uint32_t kind, uint32_t order, int CL);
+
+inline const void *search_kernel_ptr(uint32_t kind, uint32_t order, int CL, uint32_t store = 0) {
+    if (store == 1) return search_kernel_ptr_bf16(kind, order, CL);
+    if (store == 2) return search_kernel_ptr_fp8(kind, order, CL);
+    return kind == 0 ? search_kernel_ptr_fp32_ip(kind, order, CL) : search_kernel_ptr_fp32_l2(kind, order, CL);
+}
 // pss_kernel<KIND, CL> (pss_kernel.cuh); nullptr if not built.
 const void *pss_kernel_ptr(uint32_t kind, int CL);
 

@@ -1,6 +1,8 @@
 // C ABI of panns_b200 (declared in include/panns_b200.h): loaders, the HBM
 // layout of the base vectors and the graph, init-id generation, the batched
 // search launch and recall. Host code is C++; the hot path is search_kernel.cuh.
+#include <cuda_bf16.h>
+#include <cuda_fp8.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -122,6 +124,43 @@ __global__ void norms_kernel(const float *__restrict__ vec, float *__restrict__ 
     }
 }
 
+// Per-dimension absolute maximum (FP8 scales), as float bits (non-negative
+// floats order like their bit patterns).
+__global__ void absmax_kernel(const float *__restrict__ raw, uint64_t n, int d, unsigned int *amax) {
+    const uint64_t total = n * (uint64_t) d;
+    for (uint64_t t = blockIdx.x * (uint64_t) blockDim.x + threadIdx.x; t < total;
+         t += (uint64_t) gridDim.x * blockDim.x)
+        atomicMax(amax + (t % d), __float_as_uint(fabsf(raw[t])));
+}
+
+// Reduced copy, natural element order, row u = original row rowmap[u], padded
+// to dpad with zeros: BF16 (round to nearest even) or FP8 E4M3 of x / scale
+// (saturating). Then ||v^||^2 of the dequantised row.
+__global__ void quantize_rows_kernel(const float *__restrict__ raw, void *out, float *norms_lo,
+                                     uint32_t n, int d, int dpad, const uint32_t *__restrict__ rowmap,
+                                     int store, const float *__restrict__ scales) {
+    for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x) {
+        const float *x = raw + (uint64_t) rowmap[u] * d;
+        float s = 0.f;
+        for (int e = 0; e < dpad; ++e) {
+            const float v = e < d ? x[e] : 0.f;
+            float back;
+            if (store == PANNS_STORE_BF16) {
+                const __nv_bfloat16 b = __float2bfloat16_rn(v);
+                reinterpret_cast<__nv_bfloat16 *>(out)[(uint64_t) u * dpad + e] = b;
+                back = __bfloat162float(b);
+            } else {
+                const __nv_fp8_storage_t f = __nv_cvt_float_to_fp8(v / scales[e], __NV_SATFINITE, __NV_E4M3);
+                reinterpret_cast<__nv_fp8_storage_t *>(out)[(uint64_t) u * dpad + e] = f;
+                const __half_raw hr = __nv_cvt_fp8_to_halfraw(f, __NV_E4M3);
+                back = __half2float(*reinterpret_cast<const __half *>(&hr)) * scales[e];
+            }
+            s = fmaf(back, back, s);
+        }
+        norms_lo[u] = s;
+    }
+}
+
 template <typename T>
 struct DevBuf {
     T *p = nullptr;
@@ -152,6 +191,8 @@ struct panns_index {
     // base vectors (raw rows stay on the device until the index is finalised)
     uint32_t n = 0, d = 0, dpad = 0, storage = 0;
     DevBuf<float> base_raw, vec, norms;
+    DevBuf<uint8_t> vec_lo;         // reduced copy (BF16 or FP8 rows)
+    DevBuf<float> norms_lo, scales; // its norms; FP8 per-dimension scales
     bool ready = false;             // vec/norms/head built for the current base + graph
     std::vector<uint32_t> perm, inv;  // device id -> original id, and back
     DevBuf<uint32_t> orig;
@@ -233,8 +274,7 @@ int panns_set_base(panns_index *h, const float *data, uint32_t n, uint32_t d, ui
     if (d % 8) return fail(PANNS_EINVAL, "panns_set_base: d must be a multiple of 8");
     if (d > 256) return fail(PANNS_EINVAL, "panns_set_base: d > 256 is not supported");
     if (n > 0x7fffffffu) return fail(PANNS_EINVAL, "panns_set_base: n must be < 2^31");
-    if (storage != PANNS_STORE_FP32)
-        return fail(PANNS_EINVAL, "panns_set_base: only FP32 storage is available in this build");
+    if (storage > PANNS_STORE_FP8) return fail(PANNS_EINVAL, "panns_set_base: unknown storage");
     if (h->qd && h->qd != d) return fail(PANNS_EINVAL, "panns_set_base: dimension differs from the queries");
     if (h->gn && h->gn != n)
         return fail(PANNS_EINVAL, "panns_set_base: base has " + std::to_string(n) +
@@ -398,6 +438,34 @@ static int finalize(panns_index *h) {
     {
         const int blocks = std::max(1, (int) std::min<uint32_t>((n + 255) / 256, h->num_sms * 32u));
         norms_kernel<<<blocks, 256, 0, h->stream>>>(h->vec.p, h->norms.p, n, (int) h->dpad);
+        CU(cudaGetLastError());
+    }
+    if (h->storage != PANNS_STORE_FP32) {
+        const size_t esz = h->storage == PANNS_STORE_BF16 ? 2 : 1;
+        CU(h->vec_lo.ensure((size_t) n * h->dpad * esz));
+        CU(h->norms_lo.ensure(n));
+        CU(h->scales.ensure(h->dpad));
+        std::vector<float> sc(h->dpad, 1.0f);
+        if (h->storage == PANNS_STORE_FP8) {
+            DevBuf<unsigned int> amax;
+            CU(amax.ensure(h->d));
+            CU(cudaMemsetAsync(amax.p, 0, h->d * 4ull, h->stream));
+            absmax_kernel<<<h->num_sms * 8, 256, 0, h->stream>>>(h->base_raw.p, n, (int) h->d, amax.p);
+            CU(cudaGetLastError());
+            std::vector<unsigned int> am(h->d);
+            CU(cudaMemcpyAsync(am.data(), amax.p, h->d * 4ull, cudaMemcpyDeviceToHost, h->stream));
+            CU(cudaStreamSynchronize(h->stream));
+            for (uint32_t e = 0; e < h->d; ++e) {
+                float m;
+                memcpy(&m, &am[e], 4);
+                sc[e] = m > 0.f ? m / 448.0f : 1.0f;  // E4M3 largest finite value: 448
+            }
+        }
+        CU(cudaMemcpyAsync(h->scales.p, sc.data(), h->dpad * 4ull, cudaMemcpyHostToDevice, h->stream));
+        const int blocks = std::max(1, (int) std::min<uint32_t>((n + 127) / 128, h->num_sms * 16u));
+        quantize_rows_kernel<<<blocks, 128, 0, h->stream>>>(h->base_raw.p, h->vec_lo.p, h->norms_lo.p, n,
+                                                            (int) h->d, (int) h->dpad, h->orig.p,
+                                                            (int) h->storage, h->scales.p);
         CU(cudaGetLastError());
     }
     // head rows + overflow in device ids
@@ -577,6 +645,14 @@ int check_params(panns_index *h, const panns_search_params *p) {
     }
     if (p->warps_per_block > 8) return fail(PANNS_EINVAL, "search: warps_per_block must be <= 8");
     if (p->flags) return fail(PANNS_EINVAL, "search: flags must be 0");
+    if (p->storage > PANNS_STORE_FP8) return fail(PANNS_EINVAL, "search: unknown storage");
+    if (p->storage != PANNS_STORE_FP32) {
+        if (p->storage != h->storage)
+            return fail(PANNS_EINVAL, "search: that reduced copy was not built (panns_set_base storage)");
+        const bool ok = p->mode == PANNS_MODE_NSG_SEQ || p->mode == PANNS_MODE_TOP_M ||
+                        (p->mode == PANNS_MODE_PSS_V5 && p->T == 1);
+        if (!ok) return fail(PANNS_EINVAL, "search: reduced storage is for NSG_SEQ and TOP_M");
+    }
     return PANNS_OK;
 }
 
@@ -591,10 +667,14 @@ static int launch_search(panns_index *h, const panns_search_params *p, const flo
     const uint32_t order = p->mode == PANNS_MODE_EFANNA ? ORDER_EFANNA : ORDER_PANNS;
     const uint32_t kind = p->distance == PANNS_DIST_L2 ? KIND_L2 : KIND_IP;
     const bool pss = p->mode == PANNS_MODE_PSS_V5 && p->T > 1;
-    const void *kern = pss ? pss_kernel_ptr(kind, CL) : search_kernel_ptr(kind, order, CL);
+    const void *kern = pss ? pss_kernel_ptr(kind, CL) : search_kernel_ptr(kind, order, CL, p->storage);
     if (!kern) return fail(PANNS_EINVAL, "search: unsupported dimension");
     const uint32_t M = p->mode == PANNS_MODE_TOP_M ? p->M : 1u;
-    const uint32_t qcap = ((p->L + 31) / 32) * 32;
+    uint32_t qcap = ((p->L + 31) / 32) * 32;
+    if (p->storage != PANNS_STORE_FP32) {  // the re-rank sorts the queue in place
+        qcap = 32;
+        while (qcap < p->L) qcap <<= 1;
+    }
     const uint32_t L_local = p->L_local ? p->L_local : p->L;
     const uint32_t wcap = ((L_local + 31) / 32) * 32;
     uint32_t wpb = p->warps_per_block ? p->warps_per_block : 4u;
@@ -641,6 +721,10 @@ static int launch_search(panns_index *h, const panns_search_params *p, const flo
     a.ovf_off = h->ovf_off.p;
     a.ovf = h->ovf.p;
     a.orig = h->orig.p;
+    a.vec_lo = h->vec_lo.p;
+    a.norms_lo = h->norms_lo.p;
+    a.scales = h->scales.p;
+    a.d = h->d;
     a.n = h->n;
     a.queries = reinterpret_cast<const float4 *>(d_queries_cm);
     a.nq = nq;
@@ -941,7 +1025,8 @@ extern "C" int panns_search_static(panns_index *h, const panns_search_params *p,
                                       " exceeds the fixed scratch limit of " + std::to_string(kStaticMaxL));
     if (p->mode == PANNS_MODE_TOP_M && (p->M == 0 || p->M > (uint32_t) kMaxM))
         return fail(PANNS_EINVAL, "panns_search_static: TOP_M needs 1 <= M <= 64");
-    if (p->warps_per_block > 8 || p->flags) return fail(PANNS_EINVAL, "panns_search_static: bad params");
+    if (p->warps_per_block > 8 || p->flags || p->storage != PANNS_STORE_FP32)
+        return fail(PANNS_EINVAL, "panns_search_static: bad params (float32 storage only)");
     if (nq == 0) return PANNS_OK;
     if (!d_queries || !d_out_ids) return fail(PANNS_EINVAL, "panns_search_static: NULL device buffer");
     cudaStream_t st = stream ? (cudaStream_t) stream : h->stream;
@@ -1025,6 +1110,10 @@ extern "C" int panns_search_static(panns_index *h, const panns_search_params *p,
     a.ovf_off = h->ovf_off.p;
     a.ovf = h->ovf.p;
     a.orig = h->orig.p;
+    a.vec_lo = nullptr;
+    a.norms_lo = nullptr;
+    a.scales = nullptr;
+    a.d = h->d;
     a.n = h->n;
     a.queries = reinterpret_cast<const float4 *>(d_qcm);
     a.nq = nq;

@@ -43,6 +43,7 @@
 // went from zero to non-zero, so only those are cleared after the query.
 #pragma once
 
+#include <cuda_fp8.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -60,6 +61,10 @@ constexpr int kMaxM = 64;
 
 enum { ORDER_PANNS = 0, ORDER_EFANNA = 1 };
 enum { KIND_IP = 0, KIND_L2 = 1 };
+// Storage the search distances are computed from: the exact float32 rows, or
+// a reduced copy (BF16, or FP8 E4M3 with per-dimension scales) whose final L
+// candidates are re-ranked with the exact float32 distance.
+enum { STORE_FP32 = 0, STORE_BF16 = 1, STORE_FP8 = 2 };
 
 // Error bits written to SearchArgs::error.
 enum : uint32_t { ERR_BAD_ID = 1u, ERR_BAD_INIT = 2u };
@@ -85,7 +90,12 @@ struct SearchArgs {
     uint32_t dirty_cap;
     uint32_t *counter;        // work-stealing query counter
     uint32_t *error;          // ERR_* bits
-    uint32_t queue_cap;       // shared-memory queue entries per warp (>= L)
+    uint32_t queue_cap;       // shared-memory queue entries per warp (>= L; a power of
+                              // two >= L when a reduced copy is searched)
+    const void *vec_lo;       // reduced rows, natural element order: n x dpad (BF16 or FP8)
+    const float *norms_lo;    // ||v||^2 of the dequantised rows
+    const float *scales;      // FP8: per-dimension scale (dpad)
+    uint32_t d;               // dimension
 };
 
 // Bytes of shared memory one warp needs.
@@ -383,26 +393,182 @@ static __device__ __forceinline__ void note_dirty(uint32_t *dirty, uint32_t dirt
     dcount += __popc(bm);
 }
 
+// ---------------------------------------------------------------------------
+// Distance policies. distances(a, ids, out, nb): out[b] = distance of the
+// query to vertex ids[b] & kIdMask, for b < nb, computed by the whole warp.
+// ---------------------------------------------------------------------------
+template <int KIND, int CL, int STORE>
+struct Dist;
+
+// Exact float32, reference lane order (8 lanes per vertex, chain-major rows).
+template <int KIND, int CL>
+struct Dist<KIND, CL, STORE_FP32> {
+    float4 qv[CL];
+    __device__ __forceinline__ void load(const SearchArgs &a, uint32_t q, int lane) {
+        const float4 *qrow = a.queries + (size_t) q * (CL * 8);
+#pragma unroll
+        for (int i = 0; i < CL; ++i) qv[i] = __ldg(qrow + 8 * i + (lane & 7));
+    }
+    __device__ __forceinline__ void distances(const SearchArgs &a, const uint32_t *ids, float *out,
+                                              uint32_t nb, int lane) const {
+        const int g = lane >> 3;
+        // 8 vertices per round (2 per 8-lane group, loads issued together).
+        for (uint32_t b0 = 0; b0 < nb; b0 += 8) {
+            const uint32_t b = b0 + g, bb = b0 + 4 + g;
+            const bool act0 = b < nb, act1 = bb < nb;
+            const uint32_t v0 = act0 ? ids[b] & kIdMask : 0u, v1 = act1 ? ids[bb] & kIdMask : 0u;
+            float d0, d1;
+            group_distance2<KIND, CL>(a.vec, a.norms, v0, act0, v1, act1, qv, lane, d0, d1);
+            if ((lane & 7) == 0) {
+                if (act0) out[b] = d0;
+                if (act1) out[bb] = d1;
+            }
+        }
+        __syncwarp();
+    }
+};
+
+// Position of natural element e in a chain-major padded row (inverse of the
+// layout's chain_term_element).
+static __device__ __forceinline__ int chain_major_pos(int d, int e) {
+    const int DR = d % 16, DD = d - DR;
+    int c, k;
+    if (DR && e >= DD) {
+        c = e - DD;
+        k = 0;
+    } else {
+        c = e & 7;
+        k = (e >> 3) + (DR ? 1 : 0);
+    }
+    return (8 * (k >> 2) + c) * 4 + (k & 3);
+}
+
+// Reduced copy: 4 lanes per vertex, lane t of the group owns 8-element chunks
+// t, t+4, ..., t+4(CL-1) of the row; accumulation in float32; the ranking
+// distance is ||v^||^2 - 2 <v^, q> on the dequantised row v^ (the constant
+// ||q||^2 is left out, as in the norm trick). FP8 scales are folded into the
+// query once.
+template <int KIND, int CL, int STORE>
+struct Dist {
+    float ql[8 * CL];
+    __device__ __forceinline__ void load(const SearchArgs &a, uint32_t q, int lane) {
+        const float *qrow = reinterpret_cast<const float *>(a.queries) + (size_t) q * (CL * 32);
+        const int t = lane & 3;
+#pragma unroll
+        for (int i = 0; i < CL; ++i) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int e = 8 * (t + 4 * i) + j;
+                float x = e < (int) a.d ? __ldg(qrow + chain_major_pos((int) a.d, e)) : 0.f;
+                if (STORE == STORE_FP8) x *= __ldg(a.scales + e);
+                ql[8 * i + j] = x;
+            }
+        }
+    }
+    __device__ __forceinline__ float dot_row(const void *vec_lo, uint32_t v, int t) const {
+        float acc = 0.f;
+        if (STORE == STORE_BF16) {
+            const uint4 *row = reinterpret_cast<const uint4 *>(vec_lo) + (size_t) v * (CL * 4);
+            uint4 x[CL];
+#pragma unroll
+            for (int i = 0; i < CL; ++i) x[i] = __ldg(row + t + 4 * i);
+#pragma unroll
+            for (int i = 0; i < CL; ++i) {
+                const uint32_t w[4] = {x[i].x, x[i].y, x[i].z, x[i].w};
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    acc = fmaf(__uint_as_float(w[j] << 16), ql[8 * i + 2 * j], acc);
+                    acc = fmaf(__uint_as_float(w[j] & 0xffff0000u), ql[8 * i + 2 * j + 1], acc);
+                }
+            }
+        } else {
+            const uint2 *row = reinterpret_cast<const uint2 *>(vec_lo) + (size_t) v * (CL * 4);
+            uint2 x[CL];
+#pragma unroll
+            for (int i = 0; i < CL; ++i) x[i] = __ldg(row + t + 4 * i);
+#pragma unroll
+            for (int i = 0; i < CL; ++i) {
+                const uint32_t w[2] = {x[i].x, x[i].y};
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const __nv_fp8x2_storage_t pair = (__nv_fp8x2_storage_t) (w[j] >> (16 * h));
+                        const __half2_raw hr = __nv_cvt_fp8x2_to_halfraw2(pair, __NV_E4M3);
+                        const float2 f = __half22float2(*reinterpret_cast<const __half2 *>(&hr));
+                        acc = fmaf(f.x, ql[8 * i + 4 * j + 2 * h], acc);
+                        acc = fmaf(f.y, ql[8 * i + 4 * j + 2 * h + 1], acc);
+                    }
+                }
+            }
+        }
+        return acc;
+    }
+    __device__ __forceinline__ void distances(const SearchArgs &a, const uint32_t *ids, float *out,
+                                              uint32_t nb, int lane) const {
+        const int g = lane >> 2, t = lane & 3;
+        // 16 vertices per round (2 per 4-lane group, loads issued together).
+        for (uint32_t b0 = 0; b0 < nb; b0 += 16) {
+            const uint32_t b = b0 + g, bb = b0 + 8 + g;
+            const bool act0 = b < nb, act1 = bb < nb;
+            const uint32_t v0 = act0 ? ids[b] & kIdMask : 0u, v1 = act1 ? ids[bb] & kIdMask : 0u;
+            float s0 = act0 ? dot_row(a.vec_lo, v0, t) : 0.f;
+            float s1 = act1 ? dot_row(a.vec_lo, v1, t) : 0.f;
+            const float n0 = act0 ? __ldg(a.norms_lo + v0) : 0.f;
+            const float n1 = act1 ? __ldg(a.norms_lo + v1) : 0.f;
+            s0 += __shfl_xor_sync(kFull, s0, 1);
+            s1 += __shfl_xor_sync(kFull, s1, 1);
+            s0 += __shfl_xor_sync(kFull, s0, 2);
+            s1 += __shfl_xor_sync(kFull, s1, 2);
+            if (t == 0) {
+                if (act0) out[b] = fmaf(-2.f, s0, n0);
+                if (act1) out[bb] = fmaf(-2.f, s1, n1);
+            }
+        }
+        __syncwarp();
+    }
+};
+
+// Sort (qd, qi)[0..sz) by (dist, original id) in place; the arrays have room
+// for the next power of two >= sz (padding (+inf, ~0)).
+static __device__ void rank_sort(float *qd, uint32_t *qi, uint32_t sz, const uint32_t *orig, int lane) {
+    uint32_t n = 1;
+    while (n < sz) n <<= 1;
+    for (uint32_t i = sz + lane; i < n; i += 32) {
+        qd[i] = __int_as_float(0x7f800000);
+        qi[i] = kFull;
+    }
+    __syncwarp();
+    for (uint32_t k = 2; k <= n; k <<= 1) {
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t i = lane; i < n; i += 32) {
+                const uint32_t ixj = i ^ j;
+                if (ixj > i) {
+                    const float ad = qd[i], xd = qd[ixj];
+                    const uint32_t ai = qi[i], xi = qi[ixj];
+                    const uint32_t ak = ai == kFull ? kFull : (ai & kIdMask);
+                    const uint32_t xk = xi == kFull ? kFull : (xi & kIdMask);
+                    const bool up = (i & k) == 0;
+                    const bool sw = up ? key_less<ORDER_PANNS>(xd, xk, ad, ak, orig)
+                                       : key_less<ORDER_PANNS>(ad, ak, xd, xk, orig);
+                    if (sw) {
+                        qd[i] = xd; qd[ixj] = ad;
+                        qi[i] = xi; qi[ixj] = ai;
+                    }
+                }
+            }
+            __syncwarp();
+        }
+    }
+}
+
 // Compute distances of the buffered fresh vertices bi[0..nb), keep the ones
 // that can still enter the queue, sort them and merge them. Returns the merge
 // position of the best survivor or L.
-template <int KIND, int ORDER, int CL>
+template <int KIND, int ORDER, int CL, int STORE>
 __device__ uint32_t flush(const SearchArgs &a, const WarpMem &m, uint32_t nb, uint32_t *sz,
-                          bool filter, const float4 (&qv)[CL], int lane) {
-    const int g = lane >> 3;
-    // Distances, 8 vertices per round (2 per 8-lane group, loads issued together).
-    for (uint32_t b0 = 0; b0 < nb; b0 += 8) {
-        const uint32_t b = b0 + g, bb = b0 + 4 + g;
-        const bool act0 = b < nb, act1 = bb < nb;
-        const uint32_t v0 = act0 ? m.bi[b] : 0u, v1 = act1 ? m.bi[bb] : 0u;
-        float d0, d1;
-        group_distance2<KIND, CL>(a.vec, a.norms, v0, act0, v1, act1, qv, lane, d0, d1);
-        if ((lane & 7) == 0) {
-            if (act0) m.bd[b] = d0;
-            if (act1) m.bd[bb] = d1;
-        }
-    }
-    __syncwarp();
+                          bool filter, const Dist<KIND, CL, STORE> &D, int lane) {
+    D.distances(a, m.bi, m.bd, nb, lane);
     // Keep the survivors, in arrival order.
     const uint32_t L = a.L;
     const float bound = (filter && *sz >= L) ? m.qd[L - 1] : __int_as_float(0x7f800000);
@@ -436,14 +602,14 @@ __device__ uint32_t flush(const SearchArgs &a, const WarpMem &m, uint32_t nb, ui
 
 // Append this lane's fresh vertex (if any) to the buffer, flushing first when
 // a full chunk might not fit.
-template <int KIND, int ORDER, int CL>
+template <int KIND, int ORDER, int CL, int STORE>
 __device__ __forceinline__ void append_fresh(const SearchArgs &a, const WarpMem &m, uint32_t &nb,
                                              uint32_t *sz, uint32_t &nk, uint32_t &n_dist,
-                                             bool fresh, uint32_t id, const float4 (&qv)[CL],
+                                             bool fresh, uint32_t id, const Dist<KIND, CL, STORE> &D,
                                              int lane) {
     if (nb + 32 > kBuf) {
         n_dist += nb;
-        nk = min(nk, flush<KIND, ORDER, CL>(a, m, nb, sz, true, qv, lane));
+        nk = min(nk, flush<KIND, ORDER, CL, STORE>(a, m, nb, sz, true, D, lane));
         nb = 0;
     }
     const uint32_t bm = __ballot_sync(kFull, fresh);
@@ -453,16 +619,12 @@ __device__ __forceinline__ void append_fresh(const SearchArgs &a, const WarpMem 
 }
 
 // One query, run by one warp.
-template <int KIND, int ORDER, int CL>
+template <int KIND, int ORDER, int CL, int STORE>
 __device__ void search_one(const SearchArgs &a, const WarpMem &m, uint32_t q, uint32_t *vis,
                            uint32_t *dirty, int lane) {
     const uint32_t L = a.L;
-    float4 qv[CL];
-    {
-        const float4 *qrow = a.queries + (size_t) q * (CL * 8);
-#pragma unroll
-        for (int i = 0; i < CL; ++i) qv[i] = __ldg(qrow + 8 * i + (lane & 7));
-    }
+    Dist<KIND, CL, STORE> D;
+    D.load(a, q, lane);
     uint32_t dcount = 0;
     uint32_t n_dist = 0, n_expand = 0, n_edges = 0, n_iter = 0;
     uint32_t sz = 0;
@@ -485,7 +647,7 @@ __device__ void search_one(const SearchArgs &a, const WarpMem &m, uint32_t q, ui
         __syncwarp();
         if (nb > kBuf - 32 || i0 + 32 >= L) {
             n_dist += nb;
-            flush<KIND, ORDER, CL>(a, m, nb, &sz, false, qv, lane);
+            flush<KIND, ORDER, CL, STORE>(a, m, nb, &sz, false, D, lane);
             nb = 0;
         }
     }
@@ -582,7 +744,7 @@ __device__ void search_one(const SearchArgs &a, const WarpMem &m, uint32_t q, ui
                 const bool valid = id != kFull;
                 const bool fresh = valid && !(olds[ch] & (1u << (id & 31)));
                 note_dirty(dirty, a.dirty_cap, dcount, valid && olds[ch] == 0, id >> 5);
-                append_fresh<KIND, ORDER, CL>(a, m, nb, &sz, nk, n_dist, fresh, id, qv, lane);
+                append_fresh<KIND, ORDER, CL, STORE>(a, m, nb, &sz, nk, n_dist, fresh, id, D, lane);
             }
             // Rows longer than the head row: the rest from the overflow list.
             if (any_long) {
@@ -601,7 +763,7 @@ __device__ void search_one(const SearchArgs &a, const WarpMem &m, uint32_t q, ui
                         const uint32_t old = visit_issue(vis, id, valid);
                         const bool fresh = valid && !(old & (1u << (id & 31)));
                         note_dirty(dirty, a.dirty_cap, dcount, valid && old == 0, id >> 5);
-                        append_fresh<KIND, ORDER, CL>(a, m, nb, &sz, nk, n_dist, fresh, id, qv, lane);
+                        append_fresh<KIND, ORDER, CL, STORE>(a, m, nb, &sz, nk, n_dist, fresh, id, D, lane);
                     }
                 }
             }
@@ -609,12 +771,20 @@ __device__ void search_one(const SearchArgs &a, const WarpMem &m, uint32_t q, ui
         }
         if (nb) {
             n_dist += nb;
-            nk = min(nk, flush<KIND, ORDER, CL>(a, m, nb, &sz, true, qv, lane));
+            nk = min(nk, flush<KIND, ORDER, CL, STORE>(a, m, nb, &sz, true, D, lane));
             nb = 0;
         }
         k = nk <= last_k ? nk : last_k + 1;
     }
 
+    if (STORE != STORE_FP32) {
+        // Re-rank the final L with the exact float32 distance (reference lane
+        // order) and order them by (distance, original id).
+        Dist<KIND, CL, STORE_FP32> E;
+        E.load(a, q, lane);
+        E.distances(a, m.qi, m.qd, sz, lane);
+        rank_sort(m.qd, m.qi, sz, a.orig, lane);
+    }
     // Results (original ids) and counters.
     for (uint32_t i = lane; i < a.K; i += 32)
         a.out_ids[(size_t) q * a.K + i] = __ldg(a.orig + (m.qi[i] & kIdMask));
@@ -628,7 +798,7 @@ __device__ void search_one(const SearchArgs &a, const WarpMem &m, uint32_t q, ui
     __syncwarp();
 }
 
-template <int KIND, int ORDER, int CL>
+template <int KIND, int ORDER, int CL, int STORE>
 __global__ void __launch_bounds__(128, 6) search_kernel(SearchArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
     const int lane = threadIdx.x & 31;
@@ -642,7 +812,7 @@ __global__ void __launch_bounds__(128, 6) search_kernel(SearchArgs a) {
         if (lane == 0) q = atomicAdd(a.counter, 1u);
         q = __shfl_sync(kFull, q, 0);
         if (q >= a.nq) break;
-        search_one<KIND, ORDER, CL>(a, m, q, vis, dirty, lane);
+        search_one<KIND, ORDER, CL, STORE>(a, m, q, vis, dirty, lane);
     }
 }
 

@@ -39,7 +39,8 @@ class PannsError(RuntimeError):
 
 class SearchParams(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint32) for n in
-                ("mode", "distance", "K", "L", "M", "T", "L_local", "X", "warps_per_block", "flags")]
+                ("mode", "distance", "K", "L", "M", "T", "L_local", "X", "warps_per_block", "storage",
+                 "flags")]
 
 
 class Stats(ctypes.Structure):

@@ -114,15 +114,15 @@ class Index:
     # -- search ---------------------------------------------------------------
     @staticmethod
     def params(mode=N.MODE_NSG_SEQ, distance=N.DIST_NORM_IP, K=100, L=100, M=1, T=1,
-               L_local=0, X=1, warps_per_block=0) -> N.SearchParams:
-        return N.SearchParams(mode, distance, K, L, M, T, L_local, X, warps_per_block, 0)
+               L_local=0, X=1, warps_per_block=0, storage=N.STORE_FP32) -> N.SearchParams:
+        return N.SearchParams(mode, distance, K, L, M, T, L_local, X, warps_per_block, storage, 0)
 
     def search(self, queries: np.ndarray | None = None, *, K=100, L=100, mode=N.MODE_NSG_SEQ,
                distance=N.DIST_NORM_IP, M=1, T=1, L_local=0, X=1, init_ids=None,
-               q_begin=0, nq=None, warps_per_block=0):
+               q_begin=0, nq=None, warps_per_block=0, storage=N.STORE_FP32):
         """Search a batch. With ``queries`` None the loaded queries
         [q_begin, q_begin + nq) are used. Returns (ids [nq x K], stats dict)."""
-        p = self.params(mode, distance, K, L, M, T, L_local, X, warps_per_block)
+        p = self.params(mode, distance, K, L, M, T, L_local, X, warps_per_block, storage)
         st = N.Stats()
         ii = None
         if init_ids is not None:

@@ -194,3 +194,37 @@ def test_gpu_pss_workers_match_oracle(mix20k, N, T, X, Ll):
         assert bad.size == 0, f"T={T} X={X} Ll={Ll} dist={dist}: rows {bad[:8].tolist()}"
         assert st["n_dist"] == nd
     ix.close()
+
+
+@pytest.mark.parametrize("storage", [1, 2])
+def test_gpu_reduced_storage_recall_and_rerank(mix20k, N, storage):
+    """BF16 / FP8-E4M3 storage: the search runs on the reduced copy, the final
+    L are re-ranked with the exact FP32 distance. Recall@100 against the
+    float64 ground truth must stay within 0.01 of the exact search at the same
+    L, and the K results must be ordered by their exact distance, then id."""
+    from parallel_anns_b200.searching import Index
+    base, q, g = mix20k
+    G = O.Graph.from_nsg(g)
+    gt, _ = O.ground_truth(base, q, 100)
+    ix = Index(0)
+    ix.set_base(base, storage=storage)
+    ix.set_graph(g)
+    ix.set_queries(q)
+    nrm = O.norms(base)
+    for L, M in ((128, 1), (200, 4)):
+        mode = N.MODE_NSG_SEQ if M == 1 else N.MODE_TOP_M
+        exact, _ = ix.search(K=100, L=L, mode=mode, M=M)
+        red, st = ix.search(K=100, L=L, mode=mode, M=M, storage=storage)
+        r_exact, r_red = O.recall_at(exact, gt, L), O.recall_at(red, gt, L)
+        assert r_red >= r_exact - 0.01, (storage, L, M, r_red, r_exact)
+        for row, qv in zip(red[:20], q[:20]):
+            d = np.array([O.distance(base[i], qv, nrm[i], O.DIST_IP_NORM) for i in row], np.float32)
+            key = list(zip(d.tolist(), row.tolist()))
+            assert key == sorted(key)
+    # exact float32 storage requested on a reduced handle still gives exact results
+    ref, _ = O.search_top_m(base, G, q, 100, 128, 1)
+    again, _ = ix.search(K=100, L=128)
+    assert np.array_equal(again, ref)
+    with pytest.raises(N.PannsError, match="EINVAL"):
+        ix.search(K=100, L=128, storage=3 - storage)  # the other reduced copy was not built
+    ix.close()
