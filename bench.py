@@ -150,6 +150,7 @@ def bench_ours(args):
 
     from parallel_anns_b200 import native as N
     from parallel_anns_b200 import workloads
+    from parallel_anns_b200.replicas import Ranks, shard
     from parallel_anns_b200.searching import Index, recall
 
     rank, world, local = dist_env()
@@ -158,17 +159,9 @@ def bench_ours(args):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=900),
                                 device_id=torch.device("cuda", local))
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    ranks = Ranks(world, device="cuda")
+    barrier = ranks.barrier
+    max_over_ranks = ranks.max
 
     spec = workloads.spec_batched_fp32_1m(n=args.n, nq=args.nq * world)
     if rank == 0:
@@ -177,8 +170,8 @@ def bench_ours(args):
     if rank != 0:
         W = workloads.load(spec)
     q_all, gt_all = W["queries"], W["gt"]
-    qs = np.ascontiguousarray(q_all[rank * args.nq:(rank + 1) * args.nq])
-    gts = gt_all[rank * args.nq:(rank + 1) * args.nq]
+    qs = np.ascontiguousarray(q_all[shard(rank, args.nq)])
+    gts = gt_all[shard(rank, args.nq)]
     nq, d, K = qs.shape[0], qs.shape[1], 100
 
     # One handle with the BF16 copy (its float32 rows serve the exact search),
@@ -220,10 +213,8 @@ def bench_ours(args):
     choice = [head_store, best[head_store][1], best[head_store][2]]
     plain = [N.STORE_FP32, best.get(N.STORE_FP32, best[head_store])[1],
              best.get(N.STORE_FP32, best[head_store])[2]]
-    if world > 1:
-        t = torch.tensor(choice + plain, dtype=torch.int64, device="cuda")
-        dist.broadcast(t, 0)
-        choice, plain = [int(x) for x in t[:3]], [int(x) for x in t[3:]]
+    both = ranks.broadcast_ints(choice + plain, 0)
+    choice, plain = both[:3], both[3:]
     store, L, M = choice
     if rank == 0:
         log(f"operating point storage={names[store]} L={L} M={M}; plain fp32 L={plain[1]} M={plain[2]}; "
