@@ -86,7 +86,7 @@ __device__ uint32_t pss_flush(const SearchArgs &a, const PssMem &m, uint32_t nb,
             const uint32_t pos = cnt + __popc(bm & lanemask_lt());
             m.bd[pos] = d;
             m.bi[pos] = id;
-            m.bk[pos] = id;
+            m.bk[pos] = __ldg(a.orig + id);
         }
         cnt += __popc(bm);
         __syncwarp();
@@ -246,7 +246,7 @@ __device__ void pss_one(const PssArgs &pa, const PssMem &m, uint32_t q, uint32_t
                     }
                 }
                 __syncwarp();
-                for (uint32_t b = lane; b < nb; b += 32) m.bk[b] = m.bi[b];
+                for (uint32_t b = lane; b < nb; b += 32) m.bk[b] = __ldg(a.orig + m.bi[b]);
                 __syncwarp();
                 warp_sort<ORDER_PANNS>(m.bd, m.bi, m.bk, nb, a.orig, lane);
                 merge_into<ORDER_PANNS>(m.md, m.mi, &msz, L, m.bd, m.bi, m.bk, nb, a.orig, lane);

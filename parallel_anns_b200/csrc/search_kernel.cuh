@@ -255,42 +255,54 @@ __device__ __forceinline__ uint32_t fresh_rank(const float *bd, const uint32_t *
     return lo;
 }
 
-// Sort (bd, bk, bi)[0..cnt) by (dist, key). Up to 32 elements: a bitonic
-// network across the lanes in registers; more: a bitonic network in shared
-// memory (padding up to the next power of two holds (+inf, ~0)).
+// (dist, key) order of the fresh buffer: the key is the original vertex id
+// (PANNS) or the arrival index (EFANNA), distinct within a buffer, so the
+// order is total and needs no lookups.
+__device__ __forceinline__ bool plain_less(float ad, uint32_t ak, float bd, uint32_t bk) {
+    return ad < bd || (ad == bd && ak < bk);
+}
+
+// Sort (bd, bk, bi)[0..cnt) by (dist, key). Up to 64 elements: by rank (each
+// lane counts the elements that precede its own one or two, with independent
+// shuffles, then writes them to their ranks); more: a bitonic network in
+// shared memory (padding up to the next power of two holds (+inf, ~0)).
 template <int ORDER>
 __device__ void warp_sort(float *bd, uint32_t *bi, uint32_t *bk, uint32_t cnt,
                           const uint32_t *orig, int lane) {
+    (void) orig;
     if (cnt <= 1) return;
-    if (cnt <= 32) {
-        const bool have = (uint32_t) lane < cnt;
-        float d = have ? bd[lane] : __int_as_float(0x7f800000);
-        uint32_t k = have ? bk[lane] : kFull;
-        uint32_t id = have ? bi[lane] : kFull;
-#pragma unroll
-        for (int kk = 2; kk <= 32; kk <<= 1) {
-#pragma unroll
-            for (int j = kk >> 1; j > 0; j >>= 1) {
-                const float pd = __shfl_xor_sync(kFull, d, j);
-                const uint32_t pk = __shfl_xor_sync(kFull, k, j);
-                const uint32_t pid = __shfl_xor_sync(kFull, id, j);
-                const bool up = (lane & kk) == 0;
-                const bool lower = (lane & j) == 0;
-                const bool p_less = key_less<ORDER>(pd, pk, d, k, orig);
-                const bool me_less = key_less<ORDER>(d, k, pd, pk, orig);
-                const bool take = (lower == up) ? p_less : me_less;
-                if (take) {
-                    d = pd;
-                    k = pk;
-                    id = pid;
-                }
+    if (cnt <= 64) {
+        const uint32_t j0 = lane, j1 = lane + 32;
+        const bool h0 = j0 < cnt, h1 = j1 < cnt;
+        const float d0 = h0 ? bd[j0] : __int_as_float(0x7f800000);
+        const float d1 = h1 ? bd[j1] : __int_as_float(0x7f800000);
+        const uint32_t k0 = h0 ? bk[j0] : kFull, k1 = h1 ? bk[j1] : kFull;
+        const uint32_t i0 = h0 ? bi[j0] : 0u, i1 = h1 ? bi[j1] : 0u;
+        uint32_t r0 = 0, r1 = 0;
+        const bool two = cnt > 32;
+#pragma unroll 8
+        for (int src = 0; src < 32; ++src) {
+            const float sd = __shfl_sync(kFull, d0, src);
+            const uint32_t sk = __shfl_sync(kFull, k0, src);
+            r0 += plain_less(sd, sk, d0, k0);
+            r1 += plain_less(sd, sk, d1, k1);
+            if (two) {
+                const float td = __shfl_sync(kFull, d1, src);
+                const uint32_t tk = __shfl_sync(kFull, k1, src);
+                r0 += plain_less(td, tk, d0, k0);
+                r1 += plain_less(td, tk, d1, k1);
             }
         }
         __syncwarp();
-        if (have) {
-            bd[lane] = d;
-            bk[lane] = k;
-            bi[lane] = id;
+        if (h0) {
+            bd[r0] = d0;
+            bk[r0] = k0;
+            bi[r0] = i0;
+        }
+        if (h1) {
+            bd[r1] = d1;
+            bk[r1] = k1;
+            bi[r1] = i1;
         }
         __syncwarp();
         return;
@@ -311,8 +323,7 @@ __device__ void warp_sort(float *bd, uint32_t *bi, uint32_t *bk, uint32_t cnt,
                     const float ad = bd[i], xd = bd[ixj];
                     const uint32_t ak = bk[i], xk = bk[ixj];
                     const bool up = (i & k) == 0;
-                    const bool sw = up ? key_less<ORDER>(xd, xk, ad, ak, orig)
-                                       : key_less<ORDER>(ad, ak, xd, xk, orig);
+                    const bool sw = up ? plain_less(xd, xk, ad, ak) : plain_less(ad, ak, xd, xk);
                     if (sw) {
                         bd[i] = xd; bd[ixj] = ad;
                         bk[i] = xk; bk[ixj] = ak;
@@ -590,7 +601,7 @@ __device__ uint32_t flush(const SearchArgs &a, const WarpMem &m, uint32_t nb, ui
             const uint32_t pos = cnt + __popc(bm & lanemask_lt());
             m.bd[pos] = d;
             m.bi[pos] = id;
-            m.bk[pos] = ORDER == ORDER_PANNS ? id : pos;
+            m.bk[pos] = ORDER == ORDER_PANNS ? __ldg(a.orig + id) : pos;
         }
         cnt += __popc(bm);
         __syncwarp();
