@@ -188,6 +188,16 @@ int panns_search_static(panns_index *h, const panns_search_params *p, const floa
 int panns_recall(const uint32_t *result_ids, uint32_t nq, uint32_t K, const uint32_t *true_ids,
                  uint32_t true_k, uint32_t L, uint32_t at, double *out);
 
+/* Float64 brute-force ground truth on the GPU: the top-k ids (original ids)
+ * by exact squared L2 in float64, ties by id, for nq host queries (nq x d
+ * float32); out_dist (optional) gets the float64 distances. Needs the base
+ * and the graph: a search gives each query a distance bound, one float64
+ * pass over all N collects the vertices within it, and an exact sort of those
+ * gives the answer. Plays the role of tools/save_true_nearest_neighbors.cpp:16-64
+ * (which scans in float32). */
+int panns_ground_truth(panns_index *h, const float *queries, uint32_t nq, uint32_t k, uint32_t *out_ids,
+                       double *out_dist);
+
 /* Read a true-NN file (u32 nq, u32 K, then nq x K x (u32 id, f32 dist)):
  * Searching::load_true_NN (PSS.cpp:141-189). Call with ids == NULL to get
  * the sizes first; ids is nq x K, dists (optional) likewise. */

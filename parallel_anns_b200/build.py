@@ -18,7 +18,7 @@ SOURCES = [os.path.join(PKG, "csrc", f) for f in
            ("panns_abi.cu", "search_kernels_fp32_ip.cu", "search_kernels_fp32_l2.cu",
             "search_kernels_bf16.cu", "search_kernels_fp8.cu", "pss_kernels.cu")]
 DEPS = SOURCES + [os.path.join(PKG, "csrc", f) for f in
-                  ("search_kernel.cuh", "pss_kernel.cuh", "kernels.h", "search_kernels.inc")] + [
+                  ("search_kernel.cuh", "pss_kernel.cuh", "gt_kernel.cuh", "kernels.h", "search_kernels.inc")] + [
     os.path.join(ROOT, "include", "panns_b200.h"),
 ]
 

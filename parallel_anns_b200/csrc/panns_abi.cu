@@ -15,6 +15,7 @@
 
 #include "../../include/panns_b200.h"
 #include "search_kernel.cuh"
+#include "gt_kernel.cuh"
 #include "pss_kernel.cuh"
 #include "kernels.h"
 
@@ -899,6 +900,78 @@ int panns_search_device(panns_index *h, const panns_search_params *p, const floa
     (void) h; (void) p; (void) d_queries; (void) nq; (void) init_ids; (void) d_out_ids; (void) stream;
     (void) stats;
     return fail(PANNS_EINVAL, "panns_search_device: not available in this build");
+}
+
+int panns_ground_truth(panns_index *h, const float *queries, uint32_t nq, uint32_t k, uint32_t *out_ids,
+                       double *out_dist) {
+    if (!h || (nq && (!queries || !out_ids))) return fail(PANNS_EINVAL, "panns_ground_truth: NULL argument");
+    if (nq == 0) return PANNS_OK;
+    int rc = finalize(h);
+    if (rc) return rc;
+    if (k == 0 || k > h->n) return fail(PANNS_EINVAL, "panns_ground_truth: need 0 < k <= N");
+    CU(cudaSetDevice(h->device));
+    // 1. An upper bound per query: a top-M search for k results (exact FP32).
+    panns_search_params p{};
+    p.mode = PANNS_MODE_TOP_M;
+    p.distance = PANNS_DIST_L2;
+    p.K = k;
+    p.L = std::min(h->n, std::max(2 * k, 256u));
+    p.M = 8;
+    p.T = 1;
+    p.X = 1;
+    std::vector<uint32_t> sids((size_t) nq * k);
+    rc = panns_search_host(h, &p, queries, nq, nullptr, sids.data(), nullptr);
+    if (rc) return rc;
+    DevBuf<float> dq;
+    DevBuf<uint32_t> dids, dcnt;
+    DevBuf<double> dtau;
+    CU(dq.ensure((size_t) nq * h->d));
+    CU(dids.ensure((size_t) nq * k));
+    CU(dtau.ensure(nq));
+    CU(dcnt.ensure(nq));
+    CU(cudaMemcpyAsync(dq.p, queries, (size_t) nq * h->d * 4, cudaMemcpyHostToDevice, h->stream));
+    CU(cudaMemcpyAsync(dids.p, sids.data(), (size_t) nq * k * 4, cudaMemcpyHostToDevice, h->stream));
+    gt_tau_kernel<<<(nq + 3) / 4, 128, 0, h->stream>>>(h->base_raw.p, (int) h->d, dq.p, nq, dids.p, k, dtau.p);
+    CU(cudaGetLastError());
+    // 2. Collect every vertex within the bound; grow the lists if any overflowed.
+    uint32_t cap = std::max(4 * k, 64u);
+    std::vector<uint32_t> cnt(nq);
+    DevBuf<double> cd;
+    DevBuf<uint32_t> ci;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        CU(cd.ensure((size_t) nq * cap));
+        CU(ci.ensure((size_t) nq * cap));
+        CU(cudaMemsetAsync(dcnt.p, 0, nq * 4ull, h->stream));
+        dim3 grid((nq + kGtQ - 1) / kGtQ, (h->n + kGtV - 1) / kGtV);
+        gt_collect_kernel<<<grid, 256, 0, h->stream>>>(h->base_raw.p, h->n, (int) h->d, dq.p, nq, dtau.p, cap,
+                                                      dcnt.p, cd.p, ci.p);
+        CU(cudaGetLastError());
+        CU(cudaMemcpyAsync(cnt.data(), dcnt.p, nq * 4ull, cudaMemcpyDeviceToHost, h->stream));
+        CU(cudaStreamSynchronize(h->stream));
+        const uint32_t mx = *std::max_element(cnt.begin(), cnt.end());
+        if (mx <= cap) break;
+        if (attempt == 1) return fail(PANNS_EDEVICE, "panns_ground_truth: candidate lists overflowed twice");
+        cap = mx;
+    }
+    // 3. Exact (distance, id) order of each list; the first k are the answer.
+    std::vector<double> hd((size_t) nq * cap);
+    std::vector<uint32_t> hi((size_t) nq * cap);
+    CU(cudaMemcpyAsync(hd.data(), cd.p, hd.size() * 8, cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaMemcpyAsync(hi.data(), ci.p, hi.size() * 4, cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    std::vector<std::pair<double, uint32_t>> tmp;
+    for (uint32_t q = 0; q < nq; ++q) {
+        const uint32_t c = cnt[q];
+        if (c < k) return fail(PANNS_EDEVICE, "panns_ground_truth: fewer candidates than k");
+        tmp.resize(c);
+        for (uint32_t i = 0; i < c; ++i) tmp[i] = {hd[(size_t) q * cap + i], hi[(size_t) q * cap + i]};
+        std::partial_sort(tmp.begin(), tmp.begin() + k, tmp.end());
+        for (uint32_t i = 0; i < k; ++i) {
+            out_ids[(size_t) q * k + i] = tmp[i].second;
+            if (out_dist) out_dist[(size_t) q * k + i] = tmp[i].first;
+        }
+    }
+    return PANNS_OK;
 }
 
 int panns_recall(const uint32_t *result_ids, uint32_t nq, uint32_t K, const uint32_t *true_ids,

@@ -27,7 +27,7 @@ EXPORTS = [
     "panns_load_fvecs_base", "panns_set_queries", "panns_load_fvecs_queries", "panns_set_graph",
     "panns_load_nsg", "panns_info", "panns_prepare_init_ids", "panns_rand_seed",
     "panns_efanna_init_ids", "panns_search", "panns_search_host", "panns_search_device",
-    "panns_recall", "panns_load_true_nn", "panns_search_static",
+    "panns_recall", "panns_load_true_nn", "panns_search_static", "panns_ground_truth",
 ]
 
 
@@ -93,6 +93,7 @@ def load(build_if_missing: bool = True):
                                       ctypes.POINTER(Stats)]
     L.panns_recall.argtypes = [P, u32, u32, P, u32, u32, u32, ctypes.POINTER(ctypes.c_double)]
     L.panns_search_static.argtypes = [P, ctypes.POINTER(SearchParams), P, u32, P, P]
+    L.panns_ground_truth.argtypes = [P, P, u32, u32, P, P]
     L.panns_load_true_nn.argtypes = [ctypes.c_char_p, P, P, P, P]
     for name in EXPORTS:
         getattr(L, name).restype = getattr(L, name).restype or ctypes.c_int

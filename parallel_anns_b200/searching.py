@@ -142,6 +142,16 @@ class Index:
         return out, st.as_dict()
 
 
+def ground_truth(index: "Index", queries: np.ndarray, k: int = 100):
+    """Top-k original ids and float64 distances by exact brute force on the GPU."""
+    queries = np.ascontiguousarray(queries, dtype=np.float32)
+    nq = queries.shape[0]
+    ids = np.empty((nq, k), dtype=np.uint32)
+    dist = np.empty((nq, k), dtype=np.float64)
+    N.check(index._lib.panns_ground_truth(index._h, N.ptr(queries), nq, k, N.ptr(ids), N.ptr(dist)))
+    return ids, dist
+
+
 def recall(result_ids: np.ndarray, true_ids: np.ndarray, L: int, at: int = 100) -> float:
     r = np.ascontiguousarray(result_ids, dtype=np.uint32)
     t = np.ascontiguousarray(true_ids, dtype=np.uint32)

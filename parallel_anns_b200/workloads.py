@@ -6,6 +6,7 @@ queries from the same mixture; NSG-style graph with R = 50 built by
 ``datasets.build_nsg_graph`` (exact 64-NN, MRNG prune, medoid entry,
 reachability repair); ground truth = top-100 by float64 brute force.
 
+Ground truth: top-100 by float64 brute force (``panns_ground_truth`` on the GPU).
 Files are written in the reference's formats (fvecs, .nsg, true-NN) to a cache
 directory so that the reference's own binaries can read them and a second
 process on the same host reuses them.
@@ -54,8 +55,7 @@ def build(spec, device=None, log=print):
     t1 = time.time()
     g = ds.build_nsg_graph(base, R=spec["R"], knn_k=spec["knn_k"], device=device)
     t2 = time.time()
-    import torch
-    gt_ids, gt_d = ds.exact_knn(base, q, spec["gt_k"], device=device, dtype=torch.float64, block=512)
+    gt_ids, gt_d = ground_truth(base, g, q, spec["gt_k"], device)
     t3 = time.time()
     fm.write_fvecs(p["base"], base)
     fm.write_fvecs(p["query"], q)
@@ -67,6 +67,20 @@ def build(spec, device=None, log=print):
         json.dump(meta, f)
     log(f"workload {spec['name']}: built in {time.time() - t0:.1f}s {meta['build_s']}")
     return {"base": base, "queries": q, "graph": g, "gt": gt_ids, "paths": p, "meta": meta}
+
+
+def ground_truth(base, graph, queries, k, device=None):
+    """Top-k by float64 brute force: the library's GPU kernel when a GPU is
+    present (panns_ground_truth), else torch float64 on the CPU."""
+    import torch
+    if torch.cuda.is_available():
+        from .searching import Index, ground_truth as gpu_gt
+        dev = torch.device(device) if device is not None else torch.device("cuda", 0)
+        with Index(dev.index or 0) as ix:
+            ix.set_base(base)
+            ix.set_graph(graph)
+            return gpu_gt(ix, queries, k)
+    return ds.exact_knn(base, queries, k, device="cpu", dtype=torch.float64, block=512)
 
 
 def load(spec):

@@ -228,3 +228,19 @@ def test_gpu_reduced_storage_recall_and_rerank(mix20k, N, storage):
     with pytest.raises(N.PannsError, match="EINVAL"):
         ix.search(K=100, L=128, storage=3 - storage)  # the other reduced copy was not built
     ix.close()
+
+
+def test_gpu_fp64_ground_truth(mix20k):
+    """The float64 brute-force kernel returns exactly the oracle's top-100
+    (ties, if any, only where float64 distances agree to 1e-12 relative)."""
+    from parallel_anns_b200.searching import Index, ground_truth
+    base, q, g = mix20k
+    ix = gpu_index(base, g)
+    ids, dist = ground_truth(ix, q, 100)
+    ref_ids, ref_d = O.ground_truth(base, q, 100)
+    bad = np.nonzero((ids != ref_ids).any(1))[0]
+    for r in bad:
+        assert np.allclose(dist[r], ref_d[r], rtol=1e-12, atol=0), r
+    assert np.allclose(dist, ref_d, rtol=1e-12, atol=0)
+    assert bad.size <= 2
+    ix.close()
