@@ -77,8 +77,20 @@ typedef struct {
     uint32_t storage;     /* panns_storage the search distances use: FP32 (exact), or
                              the reduced copy built by panns_set_base (NSG_SEQ / TOP_M
                              only; the final L are re-ranked in exact FP32) */
-    uint32_t flags;       /* reserved, must be 0 */
+    uint32_t flags;       /* PANNS_FLAG_* bits, 0 for none */
+    const uint32_t *L_query; /* optional host array, one queue length per query of the call
+                                (K <= L_query[i] <= L; not for PSS_V5 with T > 1). NSG_SEQ,
+                                TOP_M, PSS_V5: query i searches exactly as with L = L_query[i];
+                                EFANNA: with the first L_query[i] of its L init ids. NULL = L
+                                for every query. No counterpart in the reference (one L per
+                                call, PSS.cpp:1218). */
 } panns_search_params;
+
+/* Enqueue the launch (per-call memsets, query layout and the search kernel)
+ * as a CUDA graph, captured once per launch shape and replayed while the
+ * shape and buffers stay the same: small batches then pay one graph launch
+ * instead of several API calls. Results are identical. */
+#define PANNS_FLAG_CUDA_GRAPH 1u
 
 typedef struct {
     uint64_t n_dist;      /* distance computations (count_distance_computation_) */

@@ -213,6 +213,13 @@ struct panns_index {
     DevBuf<uint4> stats;
     uint32_t vis_slots = 0, vis_words = 0, dirty_cap = 0;
     std::vector<uint4> h_stats;
+    DevBuf<uint32_t> lq;        // per-query queue lengths of the current call
+    DevBuf<uint32_t> init_def;  // default PANNS init list (device ids) for init_def_L
+    uint32_t init_def_L = 0;
+    DevBuf<float> dq;           // chain-major copy of device-pointer queries
+    // Captured launch (PANNS_FLAG_CUDA_GRAPH): replayed while its key matches.
+    cudaGraphExec_t gexec = nullptr;
+    std::vector<uint8_t> gkey;
 };
 
 extern "C" {
@@ -248,6 +255,7 @@ int panns_close(panns_index *h) {
     if (!h) return PANNS_OK;
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->gexec) cudaGraphExecDestroy(h->gexec);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -493,6 +501,7 @@ static int finalize(panns_index *h) {
     if (!ovf.empty())
         CU(cudaMemcpyAsync(h->ovf.p, ovf.data(), ovf.size() * 4, cudaMemcpyHostToDevice, h->stream));
     CU(cudaStreamSynchronize(h->stream));
+    h->init_def_L = 0;
     h->ready = true;
     return PANNS_OK;
 }
@@ -645,7 +654,9 @@ int check_params(panns_index *h, const panns_search_params *p) {
         if (Ll > 8192) return fail(PANNS_EINVAL, "search: L_local > 8192 is not supported");
     }
     if (p->warps_per_block > 8) return fail(PANNS_EINVAL, "search: warps_per_block must be <= 8");
-    if (p->flags) return fail(PANNS_EINVAL, "search: flags must be 0");
+    if (p->flags & ~PANNS_FLAG_CUDA_GRAPH) return fail(PANNS_EINVAL, "search: unknown flags");
+    if (p->L_query && p->mode == PANNS_MODE_PSS_V5 && p->T > 1)
+        return fail(PANNS_EINVAL, "search: L_query is not supported by PSS_V5 with T > 1");
     if (p->storage > PANNS_STORE_FP8) return fail(PANNS_EINVAL, "search: unknown storage");
     if (p->storage != PANNS_STORE_FP32) {
         if (p->storage != h->storage)
@@ -659,11 +670,96 @@ int check_params(panns_index *h, const panns_search_params *p) {
 
 }  // namespace
 
-// Launch the search for nq chain-major device queries; everything enqueued on `stream`.
-static int launch_search(panns_index *h, const panns_search_params *p, const float *d_queries_cm,
-                         uint32_t nq, const uint32_t *h_init, uint32_t init_count,
-                         uint32_t init_stride, uint32_t *d_out, uint4 *d_stats,
-                         cudaStream_t stream, bool time_it) {
+// What one search launch enqueues: two 4-byte memsets, the optional layout of
+// row-major device queries, and the kernel.
+struct LaunchDesc {
+    const void *kern;
+    uint32_t blocks, threads;
+    size_t smem;
+    const void *args;       // SearchArgs or PssArgs
+    size_t args_size;
+    uint32_t *counter, *error;
+    const float *rows;      // row-major queries to lay out into rows_cm (or null)
+    float *rows_cm;
+    uint32_t rows_n, d, dpad;
+};
+
+static cudaError_t enqueue_plain(const LaunchDesc &l, int num_sms, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(l.counter, 0, 4, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(l.error, 0, 4, s);
+    if (e == cudaSuccess && l.rows) {
+        const uint64_t total = (uint64_t) l.rows_n * l.dpad;
+        const int pb = (int) std::min<uint64_t>((total + 255) / 256, (uint64_t) num_sms * 32);
+        permute_rows_kernel<<<std::max(pb, 1), 256, 0, s>>>(l.rows, l.rows_cm, l.rows_n, (int) l.d,
+                                                             (int) l.dpad, nullptr);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) {
+        void *argv[] = {const_cast<void *>(l.args)};
+        e = cudaLaunchKernel(l.kern, dim3(l.blocks), dim3(l.threads), argv, l.smem, s);
+    }
+    return e;
+}
+
+// Enqueue directly, or (graph) replay the handle's captured graph of the same
+// sequence, re-capturing and updating it in place when the key changed.
+static int enqueue_launch(panns_index *h, const LaunchDesc &l, cudaStream_t s, bool graph) {
+    if (!graph) {
+        CU(enqueue_plain(l, h->num_sms, s));
+        return PANNS_OK;
+    }
+    std::vector<uint8_t> key;
+    auto put = [&key](const void *v, size_t n) {
+        key.insert(key.end(), (const uint8_t *) v, (const uint8_t *) v + n);
+    };
+    const uint64_t f[] = {(uint64_t) (uintptr_t) l.kern, l.blocks, l.threads, l.smem,
+                          (uint64_t) (uintptr_t) l.counter, (uint64_t) (uintptr_t) l.error,
+                          (uint64_t) (uintptr_t) l.rows, (uint64_t) (uintptr_t) l.rows_cm,
+                          l.rows_n, l.d, l.dpad};
+    put(f, sizeof(f));
+    put(l.args, l.args_size);  // zero-filled structs, so padding compares equal
+    if (!h->gexec || key != h->gkey) {
+        cudaGraph_t g = nullptr;
+        CU(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        const cudaError_t e = enqueue_plain(l, h->num_sms, s);
+        const cudaError_t e2 = cudaStreamEndCapture(s, &g);
+        if (e != cudaSuccess || e2 != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            CU(e != cudaSuccess ? e : e2);
+        }
+        bool updated = false;
+        if (h->gexec) {
+            cudaGraphExecUpdateResultInfo info;
+            updated = cudaGraphExecUpdate(h->gexec, g, &info) == cudaSuccess;
+            if (!updated) {
+                cudaGetLastError();
+                cudaGraphExecDestroy(h->gexec);
+                h->gexec = nullptr;
+            }
+        }
+        if (!updated) {
+            const cudaError_t ei = cudaGraphInstantiate(&h->gexec, g, 0);
+            if (ei != cudaSuccess) {
+                cudaGraphDestroy(g);
+                h->gexec = nullptr;
+                CU(ei);
+            }
+        }
+        cudaGraphDestroy(g);
+        h->gkey.swap(key);
+    }
+    CU(cudaGraphLaunch(h->gexec, s));
+    return PANNS_OK;
+}
+
+// Launch the search for nq device queries (chain-major at d_queries_cm; when
+// d_rows is set they are first laid out there from row-major d_rows), with
+// device init ids and optional per-query queue lengths; everything enqueued
+// on `stream`.
+static int launch_search(panns_index *h, const panns_search_params *p, float *d_queries_cm,
+                         const float *d_rows, uint32_t nq, const uint32_t *d_init, uint32_t init_stride,
+                         const uint32_t *d_lq, uint32_t *d_out, uint4 *d_stats, cudaStream_t stream,
+                         bool time_it) {
     const int CL = (int) (h->dpad / 32);
     const uint32_t order = p->mode == PANNS_MODE_EFANNA ? ORDER_EFANNA : ORDER_PANNS;
     const uint32_t kind = p->distance == PANNS_DIST_L2 ? KIND_L2 : KIND_IP;
@@ -693,11 +789,10 @@ static int launch_search(panns_index *h, const panns_search_params *p, const flo
     uint32_t blocks = (uint32_t) per_sm * (uint32_t) h->num_sms;
     const uint32_t need_blocks = (nq + wpb - 1) / wpb;
     blocks = std::max(1u, std::min(blocks, need_blocks));
-    const uint32_t slots = blocks * wpb;
     // Per-slot visited bitsets (bounded to 16 GiB) and dirty-word lists.
     const uint32_t vis_words = (h->n + 31) / 32;
     const uint32_t dirty_cap = 8192;
-    if ((uint64_t) slots * vis_words * 4 > (16ull << 30)) {
+    if ((uint64_t) blocks * wpb * vis_words * 4 > (16ull << 30)) {
         const uint32_t max_slots = (uint32_t) ((16ull << 30) / (vis_words * 4ull));
         blocks = std::max(1u, max_slots / wpb);
     }
@@ -711,11 +806,8 @@ static int launch_search(panns_index *h, const panns_search_params *p, const flo
     }
     CU(h->counter.ensure(1));
     CU(h->error.ensure(1));
-    CU(h->init.ensure(std::max<size_t>(init_count, 1)));
-    CU(cudaMemcpyAsync(h->init.p, h_init, (size_t) init_count * 4, cudaMemcpyHostToDevice, stream));
-    CU(cudaMemsetAsync(h->counter.p, 0, 4, stream));
-    CU(cudaMemsetAsync(h->error.p, 0, 4, stream));
     SearchArgs a;
+    memset(&a, 0, sizeof(a));
     a.vec = reinterpret_cast<const float4 *>(h->vec.p);
     a.norms = h->norms.p;
     a.head = h->head.p;
@@ -729,10 +821,11 @@ static int launch_search(panns_index *h, const panns_search_params *p, const flo
     a.n = h->n;
     a.queries = reinterpret_cast<const float4 *>(d_queries_cm);
     a.nq = nq;
-    a.init_ids = h->init.p;
+    a.init_ids = d_init;
     a.init_stride = init_stride;
     a.K = p->K;
     a.L = p->L;
+    a.Lq = d_lq;
     a.M = M;
     a.out_ids = d_out;
     a.out_stats = d_stats;
@@ -744,65 +837,111 @@ static int launch_search(panns_index *h, const panns_search_params *p, const flo
     a.error = h->error.p;
     a.queue_cap = qcap;
     PssArgs pa;
-    pa.s = a;
+    memset(&pa, 0, sizeof(pa));
+    memcpy(&pa.s, &a, sizeof(a));
     pa.T = p->T;
     pa.L_local = L_local;
     pa.X = p->X;
     pa.wcap = wcap;
-    void *args[] = {&a};
-    void *pargs[] = {&pa};
+    LaunchDesc l;
+    memset(&l, 0, sizeof(l));
+    l.kern = kern;
+    l.blocks = blocks;
+    l.threads = wpb * 32;
+    l.smem = smem;
+    l.args = pss ? (const void *) &pa : (const void *) &a;
+    l.args_size = pss ? sizeof(pa) : sizeof(a);
+    l.counter = h->counter.p;
+    l.error = h->error.p;
+    l.rows = d_rows;
+    l.rows_cm = d_queries_cm;
+    l.rows_n = nq;
+    l.d = h->d;
+    l.dpad = h->dpad;
     if (time_it) CU(cudaEventRecord(h->ev0, stream));
-    CU(cudaLaunchKernel(kern, dim3(blocks), dim3(wpb * 32), pss ? pargs : args, smem, stream));
+    int rc = enqueue_launch(h, l, stream, (p->flags & PANNS_FLAG_CUDA_GRAPH) != 0);
+    if (rc) return rc;
     if (time_it) CU(cudaEventRecord(h->ev1, stream));
     return PANNS_OK;
 }
 
-static int resolve_init(panns_index *h, const panns_search_params *p, const uint32_t *init_ids,
-                        uint32_t nq, std::vector<uint32_t> &buf, const uint32_t *&ids,
-                        uint32_t &count, uint32_t &stride) {
+// Init ids as device ids on the device: the caller's (validated: in range,
+// distinct per list), efanna2e's per-query random lists, or the default PANNS
+// list, which is built once per (layout, L) and kept on the device.
+static int stage_init(panns_index *h, const panns_search_params *p, const uint32_t *init_ids,
+                      uint32_t nq, cudaStream_t stream, const uint32_t *&d_init, uint32_t &stride) {
     const uint32_t L = p->L;
-    if (p->mode == PANNS_MODE_EFANNA) {
-        stride = L;
-        count = nq * L;
-        if (init_ids) {
-            ids = init_ids;
-        } else {
+    const bool efanna = p->mode == PANNS_MODE_EFANNA;
+    stride = efanna ? L : 0;
+    if (!efanna && !init_ids && h->init_def_L == L) {
+        d_init = h->init_def.p;
+        return PANNS_OK;
+    }
+    std::vector<uint32_t> buf;
+    const uint32_t *ids = init_ids;
+    if (!ids) {
+        if (efanna) {
             int32_t st[40];
             panns_rand_seed(st, 1);
             buf.resize((size_t) nq * L);
             int rc = panns_efanna_init_ids(h, L, nq, st, buf.data());
             if (rc) return rc;
-            ids = buf.data();
-        }
-    } else {
-        stride = 0;
-        count = L;
-        if (init_ids) {
-            ids = init_ids;
         } else {
             buf.resize(L);
             int rc = panns_prepare_init_ids(h, L, buf.data());
             if (rc) return rc;
-            ids = buf.data();
         }
+        ids = buf.data();
     }
-    // Init ids must be valid, distinct vertices (per query); they are handed
-    // to the kernel as device ids, in the same order.
-    const uint32_t groups = stride ? nq : 1;
-    std::vector<uint8_t> seen(h->n, 0);
+    // Valid, distinct vertices per list; handed over as device ids in the same order.
+    const uint32_t groups = efanna ? nq : 1;
     std::vector<uint32_t> dev((size_t) groups * L);
+    const bool by_sort = (uint64_t) groups * L * 16 < h->n;
+    std::vector<uint8_t> seen(by_sort ? 0 : h->n, 0);
+    std::vector<uint32_t> tmp;
     for (uint32_t g = 0; g < groups; ++g) {
         const uint32_t *x = ids + (size_t) g * L;
         for (uint32_t i = 0; i < L; ++i) {
             if (x[i] >= h->n) return fail(PANNS_EINVAL, "search: init id out of range");
-            if (seen[x[i]]) return fail(PANNS_EINVAL, "search: duplicate init id");
-            seen[x[i]] = 1;
             dev[(size_t) g * L + i] = h->inv[x[i]];
         }
-        for (uint32_t i = 0; i < L; ++i) seen[x[i]] = 0;
+        if (by_sort) {
+            tmp.assign(x, x + L);
+            std::sort(tmp.begin(), tmp.end());
+            if (std::adjacent_find(tmp.begin(), tmp.end()) != tmp.end())
+                return fail(PANNS_EINVAL, "search: duplicate init id");
+        } else {
+            for (uint32_t i = 0; i < L; ++i) {
+                if (seen[x[i]]) return fail(PANNS_EINVAL, "search: duplicate init id");
+                seen[x[i]] = 1;
+            }
+            for (uint32_t i = 0; i < L; ++i) seen[x[i]] = 0;
+        }
     }
-    buf.swap(dev);
-    ids = buf.data();
+    if (!efanna && !init_ids) {
+        CU(h->init_def.ensure(L));
+        CU(cudaMemcpy(h->init_def.p, dev.data(), (size_t) L * 4, cudaMemcpyHostToDevice));
+        h->init_def_L = L;
+        d_init = h->init_def.p;
+        return PANNS_OK;
+    }
+    CU(h->init.ensure(dev.size()));
+    CU(cudaMemcpyAsync(h->init.p, dev.data(), dev.size() * 4, cudaMemcpyHostToDevice, stream));
+    d_init = h->init.p;
+    return PANNS_OK;
+}
+
+// Per-query queue lengths (validated K <= L_query[i] <= L) on the device, or null.
+static int stage_lq(panns_index *h, const panns_search_params *p, uint32_t nq, cudaStream_t stream,
+                    const uint32_t *&d_lq) {
+    d_lq = nullptr;
+    if (!p->L_query) return PANNS_OK;
+    for (uint32_t i = 0; i < nq; ++i)
+        if (p->L_query[i] < p->K || p->L_query[i] > p->L)
+            return fail(PANNS_EINVAL, "search: need K <= L_query[i] <= L");
+    CU(h->lq.ensure(nq));
+    CU(cudaMemcpyAsync(h->lq.p, p->L_query, (size_t) nq * 4, cudaMemcpyHostToDevice, stream));
+    d_lq = h->lq.p;
     return PANNS_OK;
 }
 
@@ -855,15 +994,15 @@ int panns_search(panns_index *h, const panns_search_params *p, const uint32_t *i
         return PANNS_OK;
     }
     CU(cudaSetDevice(h->device));
-    std::vector<uint32_t> buf;
-    const uint32_t *ids = nullptr;
-    uint32_t count = 0, stride = 0;
-    rc = resolve_init(h, p, init_ids, nq, buf, ids, count, stride);
+    const uint32_t *d_init = nullptr, *d_lq = nullptr;
+    uint32_t stride = 0;
+    rc = stage_init(h, p, init_ids, nq, h->stream, d_init, stride);
+    if (!rc) rc = stage_lq(h, p, nq, h->stream, d_lq);
     if (rc) return rc;
     CU(h->out.ensure((size_t) nq * p->K));
     CU(h->stats.ensure(nq));
-    rc = launch_search(h, p, h->queries.p + (size_t) q_begin * h->dpad, nq, ids, count, stride, h->out.p,
-                       h->stats.p, h->stream, true);
+    rc = launch_search(h, p, h->queries.p + (size_t) q_begin * h->dpad, nullptr, nq, d_init, stride, d_lq,
+                       h->out.p, h->stats.p, h->stream, true);
     if (rc) return rc;
     return finish(h, nq, p->K, out_ids, stats, t0);
 }
@@ -880,16 +1019,20 @@ int panns_search_host(panns_index *h, const panns_search_params *p, const float 
     }
     if (!queries || !out_ids) return fail(PANNS_EINVAL, "panns_search_host: NULL argument");
     CU(cudaSetDevice(h->device));
-    std::vector<uint32_t> buf;
-    const uint32_t *ids = nullptr;
-    uint32_t count = 0, stride = 0;
-    rc = resolve_init(h, p, init_ids, nq, buf, ids, count, stride);
+    const uint32_t *d_init = nullptr, *d_lq = nullptr;
+    uint32_t stride = 0;
+    rc = stage_init(h, p, init_ids, nq, h->stream, d_init, stride);
+    if (!rc) rc = stage_lq(h, p, nq, h->stream, d_lq);
     if (rc) return rc;
-    rc = upload_chain_major(h, queries, nq, h->d, h->hq);
-    if (rc) return rc;
+    // Rows go up as they are; the chain-major layout is part of the launch.
+    CU(h->raw.ensure((size_t) nq * h->d));
+    CU(h->hq.ensure((size_t) nq * h->dpad));
+    CU(cudaMemcpyAsync(h->raw.p, queries, (size_t) nq * h->d * sizeof(float), cudaMemcpyHostToDevice,
+                       h->stream));
     CU(h->out.ensure((size_t) nq * p->K));
     CU(h->stats.ensure(nq));
-    rc = launch_search(h, p, h->hq.p, nq, ids, count, stride, h->out.p, h->stats.p, h->stream, true);
+    rc = launch_search(h, p, h->hq.p, h->raw.p, nq, d_init, stride, d_lq, h->out.p, h->stats.p, h->stream,
+                       true);
     if (rc) return rc;
     return finish(h, nq, p->K, out_ids, stats, t0);
 }
@@ -897,9 +1040,21 @@ int panns_search_host(panns_index *h, const panns_search_params *p, const float 
 int panns_search_device(panns_index *h, const panns_search_params *p, const float *d_queries,
                         uint32_t nq, const uint32_t *init_ids, uint32_t *d_out_ids, void *stream,
                         panns_stats *stats) {
-    (void) h; (void) p; (void) d_queries; (void) nq; (void) init_ids; (void) d_out_ids; (void) stream;
-    (void) stats;
-    return fail(PANNS_EINVAL, "panns_search_device: not available in this build");
+    if (!h) return fail(PANNS_EINVAL, "panns_search_device: NULL handle");
+    int rc = check_params(h, p);
+    if (rc) return rc;
+    if (stats) memset(stats, 0, sizeof(*stats));
+    if (nq == 0) return PANNS_OK;
+    if (!d_queries || !d_out_ids) return fail(PANNS_EINVAL, "panns_search_device: NULL argument");
+    CU(cudaSetDevice(h->device));
+    cudaStream_t st = stream ? (cudaStream_t) stream : h->stream;
+    const uint32_t *d_init = nullptr, *d_lq = nullptr;
+    uint32_t stride = 0;
+    rc = stage_init(h, p, init_ids, nq, st, d_init, stride);
+    if (!rc) rc = stage_lq(h, p, nq, st, d_lq);
+    if (rc) return rc;
+    CU(h->dq.ensure((size_t) nq * h->dpad));
+    return launch_search(h, p, h->dq.p, d_queries, nq, d_init, stride, d_lq, d_out_ids, nullptr, st, false);
 }
 
 int panns_ground_truth(panns_index *h, const float *queries, uint32_t nq, uint32_t k, uint32_t *out_ids,
@@ -1098,8 +1253,8 @@ extern "C" int panns_search_static(panns_index *h, const panns_search_params *p,
                                       " exceeds the fixed scratch limit of " + std::to_string(kStaticMaxL));
     if (p->mode == PANNS_MODE_TOP_M && (p->M == 0 || p->M > (uint32_t) kMaxM))
         return fail(PANNS_EINVAL, "panns_search_static: TOP_M needs 1 <= M <= 64");
-    if (p->warps_per_block > 8 || p->flags || p->storage != PANNS_STORE_FP32)
-        return fail(PANNS_EINVAL, "panns_search_static: bad params (float32 storage only)");
+    if (p->warps_per_block > 8 || p->flags || p->storage != PANNS_STORE_FP32 || p->L_query)
+        return fail(PANNS_EINVAL, "panns_search_static: bad params (float32 storage, no flags, no L_query)");
     if (nq == 0) return PANNS_OK;
     if (!d_queries || !d_out_ids) return fail(PANNS_EINVAL, "panns_search_static: NULL device buffer");
     cudaStream_t st = stream ? (cudaStream_t) stream : h->stream;
@@ -1177,6 +1332,7 @@ extern "C" int panns_search_static(panns_index *h, const panns_search_params *p,
         CU(cudaGetLastError());
     }
     SearchArgs a;
+    memset(&a, 0, sizeof(a));
     a.vec = reinterpret_cast<const float4 *>(h->vec.p);
     a.norms = h->norms.p;
     a.head = h->head.p;

@@ -96,6 +96,7 @@ struct SearchArgs {
     const float *norms_lo;    // ||v||^2 of the dequantised rows
     const float *scales;      // FP8: per-dimension scale (dpad)
     uint32_t d;               // dimension
+    const uint32_t *Lq;       // per-query queue length (K <= Lq[q] <= L), or null: L for all
 };
 
 // Bytes of shared memory one warp needs.
@@ -577,11 +578,10 @@ static __device__ void rank_sort(float *qd, uint32_t *qi, uint32_t sz, const uin
 // that can still enter the queue, sort them and merge them. Returns the merge
 // position of the best survivor or L.
 template <int KIND, int ORDER, int CL, int STORE>
-__device__ uint32_t flush(const SearchArgs &a, const WarpMem &m, uint32_t nb, uint32_t *sz,
+__device__ uint32_t flush(const SearchArgs &a, const WarpMem &m, uint32_t nb, uint32_t *sz, uint32_t L,
                           bool filter, const Dist<KIND, CL, STORE> &D, int lane) {
     D.distances(a, m.bi, m.bd, nb, lane);
     // Keep the survivors, in arrival order.
-    const uint32_t L = a.L;
     const float bound = (filter && *sz >= L) ? m.qd[L - 1] : __int_as_float(0x7f800000);
     const bool any_bound = filter && *sz >= L;
     uint32_t cnt = 0;
@@ -615,12 +615,12 @@ __device__ uint32_t flush(const SearchArgs &a, const WarpMem &m, uint32_t nb, ui
 // a full chunk might not fit.
 template <int KIND, int ORDER, int CL, int STORE>
 __device__ __forceinline__ void append_fresh(const SearchArgs &a, const WarpMem &m, uint32_t &nb,
-                                             uint32_t *sz, uint32_t &nk, uint32_t &n_dist,
+                                             uint32_t *sz, uint32_t L, uint32_t &nk, uint32_t &n_dist,
                                              bool fresh, uint32_t id, const Dist<KIND, CL, STORE> &D,
                                              int lane) {
     if (nb + 32 > kBuf) {
         n_dist += nb;
-        nk = min(nk, flush<KIND, ORDER, CL, STORE>(a, m, nb, sz, true, D, lane));
+        nk = min(nk, flush<KIND, ORDER, CL, STORE>(a, m, nb, sz, L, true, D, lane));
         nb = 0;
     }
     const uint32_t bm = __ballot_sync(kFull, fresh);
@@ -633,7 +633,7 @@ __device__ __forceinline__ void append_fresh(const SearchArgs &a, const WarpMem 
 template <int KIND, int ORDER, int CL, int STORE>
 __device__ void search_one(const SearchArgs &a, const WarpMem &m, uint32_t q, uint32_t *vis,
                            uint32_t *dirty, int lane) {
-    const uint32_t L = a.L;
+    const uint32_t L = a.Lq ? __ldg(a.Lq + q) : a.L;
     Dist<KIND, CL, STORE> D;
     D.load(a, q, lane);
     uint32_t dcount = 0;
@@ -658,7 +658,7 @@ __device__ void search_one(const SearchArgs &a, const WarpMem &m, uint32_t q, ui
         __syncwarp();
         if (nb > kBuf - 32 || i0 + 32 >= L) {
             n_dist += nb;
-            flush<KIND, ORDER, CL, STORE>(a, m, nb, &sz, false, D, lane);
+            flush<KIND, ORDER, CL, STORE>(a, m, nb, &sz, L, false, D, lane);
             nb = 0;
         }
     }
@@ -755,7 +755,7 @@ __device__ void search_one(const SearchArgs &a, const WarpMem &m, uint32_t q, ui
                 const bool valid = id != kFull;
                 const bool fresh = valid && !(olds[ch] & (1u << (id & 31)));
                 note_dirty(dirty, a.dirty_cap, dcount, valid && olds[ch] == 0, id >> 5);
-                append_fresh<KIND, ORDER, CL, STORE>(a, m, nb, &sz, nk, n_dist, fresh, id, D, lane);
+                append_fresh<KIND, ORDER, CL, STORE>(a, m, nb, &sz, L, nk, n_dist, fresh, id, D, lane);
             }
             // Rows longer than the head row: the rest from the overflow list.
             if (any_long) {
@@ -774,7 +774,7 @@ __device__ void search_one(const SearchArgs &a, const WarpMem &m, uint32_t q, ui
                         const uint32_t old = visit_issue(vis, id, valid);
                         const bool fresh = valid && !(old & (1u << (id & 31)));
                         note_dirty(dirty, a.dirty_cap, dcount, valid && old == 0, id >> 5);
-                        append_fresh<KIND, ORDER, CL, STORE>(a, m, nb, &sz, nk, n_dist, fresh, id, D, lane);
+                        append_fresh<KIND, ORDER, CL, STORE>(a, m, nb, &sz, L, nk, n_dist, fresh, id, D, lane);
                     }
                 }
             }
@@ -782,7 +782,7 @@ __device__ void search_one(const SearchArgs &a, const WarpMem &m, uint32_t q, ui
         }
         if (nb) {
             n_dist += nb;
-            nk = min(nk, flush<KIND, ORDER, CL, STORE>(a, m, nb, &sz, true, D, lane));
+            nk = min(nk, flush<KIND, ORDER, CL, STORE>(a, m, nb, &sz, L, true, D, lane));
             nb = 0;
         }
         k = nk <= last_k ? nk : last_k + 1;

@@ -37,10 +37,13 @@ class PannsError(RuntimeError):
         self.code = code
 
 
+FLAG_CUDA_GRAPH = 1
+
+
 class SearchParams(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint32) for n in
                 ("mode", "distance", "K", "L", "M", "T", "L_local", "X", "warps_per_block", "storage",
-                 "flags")]
+                 "flags")] + [("L_query", ctypes.c_void_p)]
 
 
 class Stats(ctypes.Structure):

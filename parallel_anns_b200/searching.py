@@ -114,15 +114,22 @@ class Index:
     # -- search ---------------------------------------------------------------
     @staticmethod
     def params(mode=N.MODE_NSG_SEQ, distance=N.DIST_NORM_IP, K=100, L=100, M=1, T=1,
-               L_local=0, X=1, warps_per_block=0, storage=N.STORE_FP32) -> N.SearchParams:
-        return N.SearchParams(mode, distance, K, L, M, T, L_local, X, warps_per_block, storage, 0)
+               L_local=0, X=1, warps_per_block=0, storage=N.STORE_FP32, flags=0,
+               L_query=None) -> N.SearchParams:
+        """Search parameters. ``L_query``, if given, must be a C-contiguous
+        uint32 array kept alive by the caller until the call returns."""
+        lq = None if L_query is None else L_query.ctypes.data
+        return N.SearchParams(mode, distance, K, L, M, T, L_local, X, warps_per_block, storage, flags, lq)
 
     def search(self, queries: np.ndarray | None = None, *, K=100, L=100, mode=N.MODE_NSG_SEQ,
                distance=N.DIST_NORM_IP, M=1, T=1, L_local=0, X=1, init_ids=None,
-               q_begin=0, nq=None, warps_per_block=0, storage=N.STORE_FP32):
+               q_begin=0, nq=None, warps_per_block=0, storage=N.STORE_FP32, flags=0, L_query=None):
         """Search a batch. With ``queries`` None the loaded queries
-        [q_begin, q_begin + nq) are used. Returns (ids [nq x K], stats dict)."""
-        p = self.params(mode, distance, K, L, M, T, L_local, X, warps_per_block, storage)
+        [q_begin, q_begin + nq) are used. ``L_query``: optional per-query
+        queue lengths (K <= L_query[i] <= L). Returns (ids [nq x K], stats dict)."""
+        if L_query is not None:
+            L_query = np.ascontiguousarray(L_query, dtype=np.uint32)
+        p = self.params(mode, distance, K, L, M, T, L_local, X, warps_per_block, storage, flags, L_query)
         st = N.Stats()
         ii = None
         if init_ids is not None:
@@ -140,6 +147,22 @@ class Index:
                                                 N.ptr(ii) if ii is not None else None, N.ptr(out),
                                                 ctypes.byref(st)))
         return out, st.as_dict()
+
+    def search_device(self, queries, out, *, K=100, L=100, mode=N.MODE_NSG_SEQ,
+                      distance=N.DIST_NORM_IP, M=1, T=1, L_local=0, X=1, init_ids=None,
+                      warps_per_block=0, storage=N.STORE_FP32, flags=0, L_query=None, stream=None):
+        """Asynchronous search of device queries (a torch float32 CUDA tensor,
+        nq x d) into ``out`` (a torch int32/uint32 CUDA tensor, nq x K, original
+        ids), enqueued on ``stream`` (a torch.cuda.Stream; None = the handle's
+        own stream)."""
+        if L_query is not None:
+            L_query = np.ascontiguousarray(L_query, dtype=np.uint32)
+        p = self.params(mode, distance, K, L, M, T, L_local, X, warps_per_block, storage, flags, L_query)
+        ii = None if init_ids is None else np.ascontiguousarray(init_ids, dtype=np.uint32)
+        s = None if stream is None else ctypes.c_void_p(stream.cuda_stream)
+        N.check(self._lib.panns_search_device(self._h, ctypes.byref(p), ctypes.c_void_p(queries.data_ptr()),
+                                              queries.shape[0], N.ptr(ii) if ii is not None else None,
+                                              ctypes.c_void_p(out.data_ptr()), s, None))
 
 
 def ground_truth(index: "Index", queries: np.ndarray, k: int = 100):

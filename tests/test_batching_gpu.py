@@ -1,0 +1,96 @@
+"""Batching features of the search launch, through the C ABI: per-query queue
+lengths (each query searches exactly as a call with that L would), the
+asynchronous device-pointer entry point, and the CUDA-graph-captured launch
+(replayed, updated on a new shape, identical ids). Ids are checked against the
+CPU oracle and against the ordinary host entry point."""
+import numpy as np
+import pytest
+
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def setup():
+    from parallel_anns_b200 import datasets as ds
+    from parallel_anns_b200 import native as N
+    from parallel_anns_b200.searching import Index
+    base = ds.gaussian_mixture(20000, 96, seed=401, means_seed=401)
+    q = ds.gaussian_mixture(256, 96, seed=402, means_seed=401)
+    g = ds.build_nsg_graph(base, R=50, knn_k=64, device="cpu")
+    ix = Index(0)
+    ix.set_base(base)
+    ix.set_graph(g)
+    ix.set_queries(q)
+    yield ix, N, base, q, g
+    ix.close()
+
+
+@pytest.mark.parametrize("mode,M", [(0, 1), (1, 4)])
+def test_per_query_L_equals_per_L_calls(setup, mode, M):
+    ix, N, base, q, g = setup
+    K, Lmax = 50, 300
+    Lq = np.random.default_rng(7).choice([50, 64, 100, 171, 300], size=q.shape[0]).astype(np.uint32)
+    got, st = ix.search(K=K, L=Lmax, mode=mode, M=M, L_query=Lq)
+    n_dist = 0
+    for L in np.unique(Lq):
+        sel = np.nonzero(Lq == L)[0]
+        ref, s = ix.search(q[sel], K=K, L=int(L), mode=mode, M=M)
+        assert np.array_equal(got[sel], ref), f"L={L}"
+        n_dist += s["n_dist"]
+    assert st["n_dist"] == n_dist
+    # and the oracle agrees for one group
+    G = O.Graph.from_nsg(g)
+    sel = np.nonzero(Lq == 171)[0][:20]
+    ref, _ = O.search_top_m(base, G, q[sel], K, 171, M)
+    assert np.array_equal(got[sel], ref)
+
+
+def test_per_query_L_rejects_out_of_range(setup):
+    ix, N, base, q, g = setup
+    bad = np.full(q.shape[0], 40, np.uint32)  # below K
+    with pytest.raises(N.PannsError) as e:
+        ix.search(K=50, L=100, L_query=bad)
+    assert e.value.code == -1
+    bad[:] = 101  # above L
+    with pytest.raises(N.PannsError):
+        ix.search(K=50, L=100, L_query=bad)
+    with pytest.raises(N.PannsError):
+        ix.search(K=50, L=100, mode=N.MODE_PSS_V5, T=4, L_query=np.full(q.shape[0], 60, np.uint32))
+
+
+def test_device_entry_point_and_graph_replay(setup):
+    import torch
+    ix, N, base, q, g = setup
+    ref, _ = ix.search(q, K=100, L=200, mode=N.MODE_TOP_M, M=8)
+    qd = torch.from_numpy(q).cuda()
+    s = torch.cuda.Stream()
+    for flags in (0, N.FLAG_CUDA_GRAPH, N.FLAG_CUDA_GRAPH):
+        out = torch.full((q.shape[0], 100), -1, dtype=torch.int32, device="cuda")
+        ix.search_device(qd, out, K=100, L=200, mode=N.MODE_TOP_M, M=8, flags=flags, stream=s)
+        s.synchronize()
+        assert np.array_equal(out.cpu().numpy().view(np.uint32), ref)
+    # a new shape (fewer queries, other L) updates the captured graph
+    ref2, _ = ix.search(q[:37], K=10, L=64)
+    out2 = torch.full((37, 10), -1, dtype=torch.int32, device="cuda")
+    ix.search_device(qd[:37], out2, K=10, L=64, flags=N.FLAG_CUDA_GRAPH, stream=s)
+    s.synchronize()
+    assert np.array_equal(out2.cpu().numpy().view(np.uint32), ref2)
+    # host entry point with the graph flag, repeated
+    for _ in range(2):
+        got, _ = ix.search(q, K=100, L=200, mode=N.MODE_TOP_M, M=8, flags=N.FLAG_CUDA_GRAPH)
+        assert np.array_equal(got, ref)
+
+
+def test_single_query_batches(setup):
+    """Batch size 1 through the graph-replayed device path, query by query."""
+    import torch
+    ix, N, base, q, g = setup
+    ref, _ = ix.search(q[:16], K=100, L=128)
+    qd = torch.from_numpy(q[:16]).cuda()
+    out = torch.full((16, 100), -1, dtype=torch.int32, device="cuda")
+    for i in range(16):
+        ix.search_device(qd[i:i + 1], out[i:i + 1], K=100, L=128, flags=N.FLAG_CUDA_GRAPH)
+    torch.cuda.synchronize()
+    assert np.array_equal(out.cpu().numpy().view(np.uint32), ref)
