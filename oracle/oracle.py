@@ -57,6 +57,8 @@ def lib():
         L.po_efanna_init_ids.argtypes = [P, P, u32, u32, u32, u32, P, P]
         L.po_search_top_m.argtypes = [P, P, u32, u32, P, P, P, u32, P, ctypes.c_int, u32, u32, u32,
                                       ctypes.c_int, P, P, ctypes.c_int]
+        L.po_search_top_m_lists.argtypes = [P, P, u32, u32, P, P, P, u32, P, u32, P, P, u32, u32,
+                                            ctypes.c_int, P, P, ctypes.c_int]
         L.po_search_pss.argtypes = [P, P, u32, u32, P, P, P, u32, P, u32, u32, u32, u32, u32,
                                     ctypes.c_int, P, P, ctypes.c_int]
         L.po_search_efanna.argtypes = [P, P, u32, u32, P, P, P, u32, P, u32, u32, ctypes.c_int,
@@ -160,6 +162,33 @@ def search_top_m(data, g: Graph, queries, K, L, M=1, kind=DIST_IP_NORM, init_ids
                                _threads(threads))
     if rc:
         raise ValueError(f"po_search_top_m failed ({rc})")
+    return out, int(nd[0])
+
+
+def search_top_m_lists(data, g: Graph, queries, K, Lq, M, init_lists, kind=DIST_IP_NORM, nrm=None,
+                       threads=0):
+    """Top-M search where query i starts from init_lists[i] (any length <=
+    Lq[i]; repeated ids enter once) with its own queue length Lq[i]."""
+    data, queries = _vec_args(data, queries)
+    n, d = data.shape
+    nq = queries.shape[0]
+    Lq = np.ascontiguousarray(Lq, dtype=np.uint32)
+    stride = max(1, max(len(x) for x in init_lists))
+    lists = np.zeros((nq, stride), dtype=np.uint32)
+    counts = np.zeros(nq, dtype=np.uint32)
+    for i, x in enumerate(init_lists):
+        lists[i, :len(x)] = x
+        counts[i] = len(x)
+    if kind == DIST_IP_NORM and nrm is None:
+        nrm = norms(data)
+    nrm_p = _p(nrm) if kind == DIST_IP_NORM else None
+    out = np.empty((nq, K), dtype=np.uint32)
+    nd = np.zeros(1, dtype=np.uint64)
+    rc = lib().po_search_top_m_lists(_p(data), nrm_p, n, d, _p(g.offsets), _p(g.nbrs), _p(queries), nq,
+                                     _p(lists), stride, _p(counts), _p(Lq), K, M, kind, _p(out), _p(nd),
+                                     _threads(threads))
+    if rc:
+        raise ValueError(f"po_search_top_m_lists failed ({rc})")
     return out, int(nd[0])
 
 

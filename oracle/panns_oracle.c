@@ -381,6 +381,91 @@ int po_search_top_m(const float *data, const float *norms, uint32_t n, uint32_t 
     return err ? -2 : 0;
 }
 
+/* Top-M search started from a per-query init list of any length <= its own
+ * queue length L_q (the learned-entry search of panns_b200; no reference
+ * counterpart). Repeated init ids enter once; while the queue holds fewer
+ * than L_q candidates nothing is rejected, afterwards a neighbour is rejected
+ * when dist > the L_q-th distance, as in expand(). Otherwise the step of
+ * search_top_m_one. */
+static void search_top_m_list_one(ctx_t *c, const uint32_t *init, uint32_t n_init, uint32_t K,
+                                  uint32_t L, uint32_t M, cand_t *q, uint32_t *top, uint32_t *out) {
+    uint32_t size = 0;
+    for (uint32_t i = 0; i < n_init && size < L; ++i) {
+        if (test_and_set(c->visited, init[i])) continue;
+        q[size].id = init[i];
+        q[size].dist = vdist(c->data, c->norms, c->d, init[i], c->q, c->kind);
+        q[size].checked = 0;
+        ++size;
+        ++c->ndist;
+    }
+    qsort(q, size, sizeof(cand_t), cmp_cand);
+    uint32_t k = 0;
+    for (;;) {
+        uint32_t last_k = L, cnt = 0;
+        for (uint32_t i = k; i < size && cnt < M; ++i) {
+            if (q[i].checked) continue;
+            last_k = i;
+            q[i].checked = 1;
+            top[cnt++] = q[i].id;
+        }
+        if (!cnt) break;
+        uint32_t nk = L;
+        for (uint32_t j = 0; j < cnt; ++j) {
+            const uint32_t cand = top[j];
+            for (uint64_t e = c->off[cand]; e < c->off[cand + 1]; ++e) {
+                const uint32_t nb = c->nbrs[e];
+                if (test_and_set(c->visited, nb)) continue;
+                const float dist = vdist(c->data, c->norms, c->d, nb, c->q, c->kind);
+                ++c->ndist;
+                if (size >= L && dist > q[L - 1].dist) continue;
+                cand_t cc = {nb, dist, 0};
+                const uint32_t r = add_into_queue(q, &size, L, cc);
+                if (r < nk) nk = r;
+            }
+        }
+        k = nk <= last_k ? nk : last_k + 1;
+    }
+    for (uint32_t i = 0; i < K; ++i) out[i] = i < size ? q[i].id : 0xffffffffu;
+}
+
+int po_search_top_m_lists(const float *data, const float *norms, uint32_t n, uint32_t d,
+                          const uint64_t *offsets, const uint32_t *nbrs, const float *queries,
+                          uint32_t nq, const uint32_t *init_lists, uint32_t list_stride,
+                          const uint32_t *init_counts, const uint32_t *Lq, uint32_t K, uint32_t M,
+                          int kind, uint32_t *out_ids, uint64_t *out_ndist, int threads) {
+    if (M == 0 || d % 8) return -1;
+    uint32_t Lmax = 0;
+    for (uint32_t i = 0; i < nq; ++i) {
+        if (Lq[i] < K || Lq[i] > n || init_counts[i] > list_stride) return -1;
+        if (Lq[i] > Lmax) Lmax = Lq[i];
+    }
+    uint64_t total = 0;
+    int err = 0;
+#pragma omp parallel num_threads(threads > 0 ? threads : 1) reduction(+ : total) reduction(| : err)
+    {
+        ctx_t c;
+        cand_t *q = (cand_t *) malloc((size_t) (Lmax + 1) * sizeof(cand_t));
+        uint32_t *top = (uint32_t *) malloc((size_t) M * sizeof(uint32_t));
+        if (prep_ctx(&c, data, norms, n, d, offsets, nbrs, kind) || !q || !top) {
+            err |= 1;
+        } else {
+#pragma omp for schedule(dynamic, 4)
+            for (uint32_t i = 0; i < nq; ++i) {
+                c.q = queries + (size_t) i * d;
+                search_top_m_list_one(&c, init_lists + (size_t) i * list_stride, init_counts[i], K, Lq[i],
+                                      M, q, top, out_ids + (size_t) i * K);
+                memset(c.visited, 0, ((n + 63) / 64) * sizeof(uint64_t));
+            }
+        }
+        total += c.ndist;
+        free(c.visited);
+        free(q);
+        free(top);
+    }
+    if (out_ndist) *out_ndist = total;
+    return err ? -2 : 0;
+}
+
 /* PSS_v5: core/Searching.202102022027.PSS_v5.dist_thresh.profiling.cpp:1218-1515
  * (LG twin :1376-1726 adds a per-stage snapshot bound that is never tighter
  * than the live master bound, so it filters nothing extra). The parallel

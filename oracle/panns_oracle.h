@@ -64,6 +64,13 @@ int po_search_top_m(const float *data, const float *norms, uint32_t n, uint32_t 
 /* PSS_v5 with T queues (T-1 workers + master), L_local, X sub-iterations, in
  * the deterministic round-robin schedule (one expansion per worker per round,
  * workers in id order, master last). T = 1 equals po_search_top_m with M = 1. */
+/* Top-M search from per-query init lists of any length (<= list_stride),
+ * queue length Lq[i] per query; repeated init ids enter once. */
+int po_search_top_m_lists(const float *data, const float *norms, uint32_t n, uint32_t d,
+                          const uint64_t *offsets, const uint32_t *nbrs, const float *queries,
+                          uint32_t nq, const uint32_t *init_lists, uint32_t list_stride,
+                          const uint32_t *init_counts, const uint32_t *Lq, uint32_t K, uint32_t M,
+                          int kind, uint32_t *out_ids, uint64_t *out_ndist, int threads);
 int po_search_pss(const float *data, const float *norms, uint32_t n, uint32_t d,
                   const uint64_t *offsets, const uint32_t *nbrs,
                   const float *queries, uint32_t nq, const uint32_t *init_ids,

@@ -1,0 +1,32 @@
+// Host-side launchers of the learned-entry part (learned.cu), used by the
+// index code in panns_abi.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+namespace panns {
+
+// Records `msg` as the calling thread's last error (panns_last_error) and
+// returns `code`.
+int set_error(int code, const std::string &msg);
+
+// Lloyd's k-means on n row-major float32 rows of width d (device), k
+// centroids initialised from k distinct rows chosen by `seed`. On return
+// (enqueued on `stream`, synchronised): centroids (k x d, device), assign[i]
+// = cell of row i (device), rep[c] = the row of cell c nearest to its
+// centroid (device; cells left empty get a row no other cell uses).
+// Returns a PANNS_* status.
+int kmeans_run(const float *rows, uint32_t n, uint32_t d, uint32_t k, uint32_t iters, uint32_t seed,
+               float *centroids, uint32_t *assign, uint32_t *rep, cudaStream_t stream);
+
+// Packs the float32 training parameters (layout of panns_mlp_param_count)
+// into the inference layout read by mlp_prologue: BF16 w1 (d x 256),
+// w2 (256 x 256), w3 (256 x R) into `wbf` (device, 256 (d + 256 + R)
+// elements) and float32 b1, b2, b3, wl, bl into `fb` (device, 256 * 3 + R + 1).
+int mlp_pack_inference(const float *params_dev, uint32_t d, uint32_t R, void *wbf, float *fb,
+                       cudaStream_t stream);
+
+}  // namespace panns

@@ -14,6 +14,8 @@
 #include <vector>
 
 #include "../../include/panns_b200.h"
+#include "../../include/panns_learned.h"
+#include "learned.h"
 #include "search_kernel.cuh"
 #include "gt_kernel.cuh"
 #include "pss_kernel.cuh"
@@ -184,6 +186,8 @@ struct DevBuf {
 
 }  // namespace
 
+int panns::set_error(int code, const std::string &msg) { return fail(code, msg); }
+
 struct panns_index {
     int device = 0;
     int num_sms = 0;
@@ -220,6 +224,16 @@ struct panns_index {
     // Captured launch (PANNS_FLAG_CUDA_GRAPH): replayed while its key matches.
     cudaGraphExec_t gexec = nullptr;
     std::vector<uint8_t> gkey;
+    // Learned entry / L-budget network (PANNS_FLAG_LEARNED).
+    bool has_mlp = false;
+    MlpDev mlp{};                  // host copy of the device struct
+    DevBuf<uint8_t> mlp_dev;       // the struct on the device
+    DevBuf<uint16_t> mlp_w;        // BF16 weights, inference layout
+    DevBuf<float> mlp_f;           // biases and regressor
+    DevBuf<uint32_t> mlp_rep;      // representatives (device ids)
+    DevBuf<float> mlp_logits;      // slots x R
+    DevBuf<uint32_t> mlp_record;   // per query of the last call
+    uint32_t mlp_slots = 0, mlp_rec_cap = 0, mlp_last_nq = 0;
 };
 
 extern "C" {
@@ -654,7 +668,13 @@ int check_params(panns_index *h, const panns_search_params *p) {
         if (Ll > 8192) return fail(PANNS_EINVAL, "search: L_local > 8192 is not supported");
     }
     if (p->warps_per_block > 8) return fail(PANNS_EINVAL, "search: warps_per_block must be <= 8");
-    if (p->flags & ~PANNS_FLAG_CUDA_GRAPH) return fail(PANNS_EINVAL, "search: unknown flags");
+    if (p->flags & ~(PANNS_FLAG_CUDA_GRAPH | PANNS_FLAG_LEARNED)) return fail(PANNS_EINVAL, "search: unknown flags");
+    if (p->flags & PANNS_FLAG_LEARNED) {
+        if (!h->has_mlp) return fail(PANNS_ESTATE, "search: PANNS_FLAG_LEARNED without a network (panns_set_learned)");
+        const bool ok = p->mode == PANNS_MODE_NSG_SEQ || p->mode == PANNS_MODE_TOP_M ||
+                        (p->mode == PANNS_MODE_PSS_V5 && p->T == 1);
+        if (!ok) return fail(PANNS_EINVAL, "search: PANNS_FLAG_LEARNED is for NSG_SEQ, TOP_M and PSS_V5 at T = 1");
+    }
     if (p->L_query && p->mode == PANNS_MODE_PSS_V5 && p->T > 1)
         return fail(PANNS_EINVAL, "search: L_query is not supported by PSS_V5 with T > 1");
     if (p->storage > PANNS_STORE_FP8) return fail(PANNS_EINVAL, "search: unknown storage");
@@ -806,8 +826,32 @@ static int launch_search(panns_index *h, const panns_search_params *p, float *d_
     }
     CU(h->counter.ensure(1));
     CU(h->error.ensure(1));
+    const bool learned = (p->flags & PANNS_FLAG_LEARNED) != 0;
+    if (learned) {
+        // Scratch of the prologue sized for this launch; the device struct is
+        // re-uploaded (synchronously, outside any capture) when it changes.
+        bool changed = false;
+        if (h->mlp_slots < nslots) {
+            CU(h->mlp_logits.ensure((size_t) nslots * h->mlp.R));
+            h->mlp_slots = nslots;
+            changed = true;
+        }
+        if (h->mlp_rec_cap < nq) {
+            CU(h->mlp_record.ensure((size_t) nq * kMlpRecWords));
+            h->mlp_rec_cap = nq;
+            changed = true;
+        }
+        if (changed) {
+            h->mlp.logits = h->mlp_logits.p;
+            h->mlp.record = h->mlp_record.p;
+            CU(cudaStreamSynchronize(stream));
+            CU(cudaMemcpy(h->mlp_dev.p, &h->mlp, sizeof(MlpDev), cudaMemcpyHostToDevice));
+        }
+        h->mlp_last_nq = nq;
+    }
     SearchArgs a;
     memset(&a, 0, sizeof(a));
+    a.mlp = learned ? reinterpret_cast<const MlpDev *>(h->mlp_dev.p) : nullptr;
     a.vec = reinterpret_cast<const float4 *>(h->vec.p);
     a.norms = h->norms.p;
     a.head = h->head.p;
@@ -1367,5 +1411,105 @@ extern "C" int panns_search_static(panns_index *h, const panns_search_params *p,
     CU(cudaStreamSynchronize(st));
     if (err & ERR_BAD_ID) return fail(PANNS_EDEVICE, "panns_search_static: a neighbour id >= N");
     if (err & ERR_BAD_INIT) return fail(PANNS_EDEVICE, "panns_search_static: init id >= N");
+    return PANNS_OK;
+}
+
+// ---- learned entry / L budget -----------------------------------------------
+
+extern "C" int panns_kmeans(panns_index *h, uint32_t k, uint32_t iters, uint32_t seed, uint32_t *rep_ids,
+                            uint32_t *assign, float *centroids) {
+    if (!h) return fail(PANNS_EINVAL, "panns_kmeans: NULL handle");
+    if (!h->n || !h->base_raw.p) return fail(PANNS_ESTATE, "panns_kmeans: no base vectors loaded");
+    CU(cudaSetDevice(h->device));
+    DevBuf<float> cent;
+    DevBuf<uint32_t> as, rep;
+    CU(cent.ensure((size_t) k * h->d));
+    CU(as.ensure(h->n));
+    CU(rep.ensure(k));
+    int rc = panns::kmeans_run(h->base_raw.p, h->n, h->d, k, iters, seed, cent.p, as.p, rep.p, h->stream);
+    if (rc) return rc;
+    if (rep_ids) CU(cudaMemcpyAsync(rep_ids, rep.p, k * 4ull, cudaMemcpyDeviceToHost, h->stream));
+    if (assign) CU(cudaMemcpyAsync(assign, as.p, h->n * 4ull, cudaMemcpyDeviceToHost, h->stream));
+    if (centroids)
+        CU(cudaMemcpyAsync(centroids, cent.p, (size_t) k * h->d * 4, cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    return PANNS_OK;
+}
+
+extern "C" int panns_set_learned(panns_index *h, const float *params, uint32_t R, const uint32_t *rep_ids,
+                                 const panns_learned_params *lp) {
+    if (!h || !params || !rep_ids || !lp) return fail(PANNS_EINVAL, "panns_set_learned: NULL argument");
+    int rc = finalize(h);
+    if (rc) return rc;
+    if (R == 0 || R > (uint32_t) kMlpMaxR || R % kMlpH)
+        return fail(PANNS_EINVAL, "panns_set_learned: need R a multiple of 256, R <= 1024");
+    if (lp->E > (uint32_t) kMlpMaxE) return fail(PANNS_EINVAL, "panns_set_learned: need E <= 64");
+    if (!(lp->min_conf >= 0.f && lp->min_conf <= 1.f))
+        return fail(PANNS_EINVAL, "panns_set_learned: need 0 <= min_conf <= 1");
+    if (lp->use_L && !(lp->L_scale > 0.f)) return fail(PANNS_EINVAL, "panns_set_learned: need L_scale > 0");
+    std::vector<uint32_t> rep(R);
+    for (uint32_t i = 0; i < R; ++i) {
+        if (rep_ids[i] >= h->n) return fail(PANNS_EINVAL, "panns_set_learned: representative id >= N");
+        rep[i] = h->inv[rep_ids[i]];
+    }
+    CU(cudaSetDevice(h->device));
+    const uint64_t P = panns_mlp_param_count(h->d, R);
+    DevBuf<float> dp;
+    CU(dp.ensure(P));
+    CU(cudaMemcpy(dp.p, params, P * 4, cudaMemcpyHostToDevice));
+    CU(h->mlp_w.ensure((size_t) kMlpH * (h->d + kMlpH + R)));
+    CU(h->mlp_f.ensure(3u * kMlpH + R + 1));
+    CU(h->mlp_rep.ensure(R));
+    CU(h->mlp_dev.ensure(sizeof(MlpDev)));
+    rc = panns::mlp_pack_inference(dp.p, h->d, R, h->mlp_w.p, h->mlp_f.p, h->stream);
+    if (rc) return rc;
+    CU(cudaMemcpyAsync(h->mlp_rep.p, rep.data(), R * 4ull, cudaMemcpyHostToDevice, h->stream));
+    float bl = 0.f;
+    CU(cudaMemcpyAsync(&bl, h->mlp_f.p + 3u * kMlpH + R, 4, cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    MlpDev m{};
+    const __nv_bfloat16 *wb = reinterpret_cast<const __nv_bfloat16 *>(h->mlp_w.p);
+    m.w1 = wb;
+    m.w2 = wb + (size_t) h->d * kMlpH;
+    m.w3 = wb + (size_t) (h->d + kMlpH) * kMlpH;
+    m.b1 = h->mlp_f.p;
+    m.b2 = h->mlp_f.p + kMlpH;
+    m.b3 = h->mlp_f.p + 2 * kMlpH;
+    m.wl = h->mlp_f.p + 2 * kMlpH + R;
+    m.bl = bl;
+    m.rep = h->mlp_rep.p;
+    m.d = h->d;
+    m.R = R;
+    m.E = lp->E;
+    m.L_init = lp->L_init;
+    m.L_min = lp->L_min;
+    m.use_entry = lp->E > 0;
+    m.use_L = lp->use_L;
+    m.min_conf = lp->min_conf;
+    m.L_scale = lp->L_scale;
+    m.logits = h->mlp_logits.p;
+    m.record = h->mlp_record.p;
+    if (h->mlp_slots && h->mlp_logits.n < (size_t) h->mlp_slots * R) {  // R grew: re-size at the next launch
+        h->mlp_slots = 0;
+        m.logits = nullptr;
+    }
+    h->mlp = m;
+    CU(cudaMemcpy(h->mlp_dev.p, &h->mlp, sizeof(MlpDev), cudaMemcpyHostToDevice));
+    h->has_mlp = true;
+    return PANNS_OK;
+}
+
+extern "C" int panns_learned_record(panns_index *h, uint32_t nq, uint32_t *out) {
+    if (!h || (nq && !out)) return fail(PANNS_EINVAL, "panns_learned_record: NULL argument");
+    if (nq > h->mlp_last_nq) return fail(PANNS_EINVAL, "panns_learned_record: nq exceeds the last learned call");
+    if (nq == 0) return PANNS_OK;
+    CU(cudaSetDevice(h->device));
+    CU(cudaStreamSynchronize(h->stream));
+    CU(cudaMemcpy(out, h->mlp_record.p, (size_t) nq * kMlpRecWords * 4, cudaMemcpyDeviceToHost));
+    for (uint32_t q = 0; q < nq; ++q) {  // entries as original ids
+        uint32_t *r = out + (size_t) q * kMlpRecWords;
+        const uint32_t E = std::min<uint32_t>(r[1], kMlpMaxE);
+        for (uint32_t i = 0; i < E; ++i) r[2 + i] = r[2 + i] < h->n ? h->perm[r[2 + i]] : r[2 + i];
+    }
     return PANNS_OK;
 }

@@ -47,6 +47,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "mlp_infer.cuh"
+
 namespace panns {
 
 constexpr uint32_t kChecked = 0x80000000u;
@@ -97,6 +99,7 @@ struct SearchArgs {
     const float *scales;      // FP8: per-dimension scale (dpad)
     uint32_t d;               // dimension
     const uint32_t *Lq;       // per-query queue length (K <= Lq[q] <= L), or null: L for all
+    const MlpDev *mlp;        // entry / L-budget network run in the prologue, or null
 };
 
 // Bytes of shared memory one warp needs.
@@ -631,32 +634,44 @@ __device__ __forceinline__ void append_fresh(const SearchArgs &a, const WarpMem 
 
 // One query, run by one warp.
 template <int KIND, int ORDER, int CL, int STORE>
-__device__ void search_one(const SearchArgs &a, const WarpMem &m, uint32_t q, uint32_t *vis,
+__device__ void search_one(const SearchArgs &a, const WarpMem &m, uint32_t q, uint32_t slot, uint32_t *vis,
                            uint32_t *dirty, int lane) {
-    const uint32_t L = a.Lq ? __ldg(a.Lq + q) : a.L;
+    uint32_t L = a.Lq ? __ldg(a.Lq + q) : a.L;
+    // Init ids: n_lrn learned entries (m.cand) then n_plain of the init list.
+    uint32_t n_lrn = 0, n_plain = L;
+    if (ORDER == ORDER_PANNS && a.mlp) {
+        const uint2 r = mlp_prologue(a.mlp, reinterpret_cast<const float *>(a.queries) + (size_t) q * CL * 32,
+                                     L, a.K, slot, q, m.cand, lane);
+        n_lrn = r.x & 0xffu;
+        n_plain = r.x >> 8;
+        L = r.y;
+    }
     Dist<KIND, CL, STORE> D;
     D.load(a, q, lane);
     uint32_t dcount = 0;
     uint32_t n_dist = 0, n_expand = 0, n_edges = 0, n_iter = 0;
     uint32_t sz = 0;
 
-    // Initial queue: the L init ids, all marked visited, sorted (init order
-    // breaks equal distances for efanna2e).
+    // Initial queue: the init ids, all marked visited, sorted (init order
+    // breaks equal distances for efanna2e). A repeated id (a learned entry
+    // that is also in the init list) enters once.
     const uint32_t *init = a.init_ids + (size_t) q * a.init_stride;
+    const uint32_t n_init = n_lrn + n_plain;
     uint32_t nb = 0;
-    for (uint32_t i0 = 0; i0 < L; i0 += 32) {
+    for (uint32_t i0 = 0; i0 < n_init; i0 += 32) {
         const uint32_t i = i0 + lane;
-        const bool valid = i < L;
-        uint32_t id = valid ? __ldg(init + i) : 0u;
+        const bool valid = i < n_init;
+        uint32_t id = valid ? (i < n_lrn ? m.cand[i] : __ldg(init + (i - n_lrn))) : 0u;
         const bool ok = valid && id < a.n;
         if (valid && !ok) atomicOr(a.error, ERR_BAD_INIT);
         const uint32_t old = visit_issue(vis, id, ok);
         note_dirty(dirty, a.dirty_cap, dcount, ok && old == 0, id >> 5);
-        const uint32_t bm = __ballot_sync(kFull, ok);
-        if (ok) m.bi[nb + __popc(bm & lanemask_lt())] = id;
+        const bool fresh = ok && !(old & (1u << (id & 31)));
+        const uint32_t bm = __ballot_sync(kFull, fresh);
+        if (fresh) m.bi[nb + __popc(bm & lanemask_lt())] = id;
         nb += __popc(bm);
         __syncwarp();
-        if (nb > kBuf - 32 || i0 + 32 >= L) {
+        if (nb > kBuf - 32 || i0 + 32 >= n_init) {
             n_dist += nb;
             flush<KIND, ORDER, CL, STORE>(a, m, nb, &sz, L, false, D, lane);
             nb = 0;
@@ -823,7 +838,7 @@ __global__ void __launch_bounds__(128, 6) search_kernel(SearchArgs a) {
         if (lane == 0) q = atomicAdd(a.counter, 1u);
         q = __shfl_sync(kFull, q, 0);
         if (q >= a.nq) break;
-        search_one<KIND, ORDER, CL, STORE>(a, m, q, vis, dirty, lane);
+        search_one<KIND, ORDER, CL, STORE>(a, m, q, slot, vis, dirty, lane);
     }
 }
 

@@ -28,6 +28,9 @@ EXPORTS = [
     "panns_load_nsg", "panns_info", "panns_prepare_init_ids", "panns_rand_seed",
     "panns_efanna_init_ids", "panns_search", "panns_search_host", "panns_search_device",
     "panns_recall", "panns_load_true_nn", "panns_search_static", "panns_ground_truth",
+    # include/panns_learned.h
+    "panns_mlp_param_count", "panns_mlp_loss_grad", "panns_mlp_forward", "panns_mlp_train",
+    "panns_kmeans", "panns_set_learned", "panns_learned_record",
 ]
 
 
@@ -38,12 +41,23 @@ class PannsError(RuntimeError):
 
 
 FLAG_CUDA_GRAPH = 1
+FLAG_LEARNED = 2
 
 
 class SearchParams(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint32) for n in
                 ("mode", "distance", "K", "L", "M", "T", "L_local", "X", "warps_per_block", "storage",
                  "flags")] + [("L_query", ctypes.c_void_p)]
+
+
+class MlpTrainParams(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint32) for n in ("d", "R", "T", "batch", "epochs", "seed")] + [
+        (n, ctypes.c_float) for n in ("lr", "beta1", "beta2", "eps", "weight_decay", "lambda_L")]
+
+
+class LearnedParams(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint32) for n in ("E", "L_init", "L_min", "use_L")] + [
+        (n, ctypes.c_float) for n in ("L_scale", "min_conf")]
 
 
 class Stats(ctypes.Structure):
@@ -98,6 +112,15 @@ def load(build_if_missing: bool = True):
     L.panns_search_static.argtypes = [P, ctypes.POINTER(SearchParams), P, u32, P, P]
     L.panns_ground_truth.argtypes = [P, P, u32, u32, P, P]
     L.panns_load_true_nn.argtypes = [ctypes.c_char_p, P, P, P, P]
+    L.panns_mlp_param_count.argtypes = [u32, u32]
+    L.panns_mlp_param_count.restype = ctypes.c_uint64
+    L.panns_mlp_loss_grad.argtypes = [i32, u32, u32, u32, P, P, P, P, u32, ctypes.c_float, P,
+                                      ctypes.POINTER(ctypes.c_double)]
+    L.panns_mlp_forward.argtypes = [i32, u32, u32, P, P, u32, P]
+    L.panns_mlp_train.argtypes = [i32, ctypes.POINTER(MlpTrainParams), P, P, P, u32, P, P]
+    L.panns_kmeans.argtypes = [P, u32, u32, u32, P, P, P]
+    L.panns_set_learned.argtypes = [P, P, u32, P, ctypes.POINTER(LearnedParams)]
+    L.panns_learned_record.argtypes = [P, u32, P]
     for name in EXPORTS:
         getattr(L, name).restype = getattr(L, name).restype or ctypes.c_int
     L.panns_last_error.restype = ctypes.c_char_p
