@@ -3,10 +3,16 @@
 
 Workload (batched FP32): N = 1,000,000 base vectors, d = 96, 64-component
 Gaussian mixture (sigma 0.3, unit norm), NSG-style graph R = 50; 10,000
-queries per GPU (weak scaling: rank r searches its own 10,000); K = 100.
-Metric: queries per second at recall@100 >= 0.95 (the smallest L of the
-sweep that reaches it, per M; the fastest (L, M) wins — the reference's
-"lowest runtime with P@100 >= target" rule).
+evaluation queries per GPU (weak scaling: rank r searches its own 10,000);
+K = 100. Metric: queries per second at recall@100 >= 0.95.
+
+Operating points are chosen by the autotuner (parallel_anns_b200/autotune.py)
+on 10,000 held-out tuning queries of another seed, never on the evaluated
+ones: per candidate (storage FP32 / BF16 / FP8, with or without the learned
+entry network, M) the smallest L reaching the target, then the warps per
+block; the fastest wins ("value"), and the plain FP32 search is tuned and
+reported beside it ("plain_fp32"). The learned network is trained on the GPU
+on 200,000 held-out queries before tuning (cached with the workload).
 
 One step = one batched search of all of a rank's queries (one kernel launch).
 ``value``: device time of the search kernel (CUDA events) with base, graph
@@ -14,6 +20,8 @@ and queries resident in HBM; the 384 MB base set alone is larger than L2 and
 L2 is also flushed (a 256 MB write) before every step.
 ``e2e``: the same search through the C ABI's host-pointer entry point
 (panns_search_host: queries copied host->device, ids copied back), wall time.
+``batching``: batches of 1, 64 and 1,000 queries back to back through the
+asynchronous device-pointer entry point with the CUDA-graph-captured launch.
 
 ``--impl reference`` times the reference's own PSS_v5
 (core/Searching.202102022027.PSS_v5.dist_thresh.profiling.cpp, built from its
@@ -148,6 +156,8 @@ def bench_ours(args):
     import torch
     import torch.distributed as dist
 
+    from parallel_anns_b200 import autotune as AT
+    from parallel_anns_b200 import learned as LE
     from parallel_anns_b200 import native as N
     from parallel_anns_b200 import workloads
     from parallel_anns_b200.replicas import Ranks, shard
@@ -166,9 +176,11 @@ def bench_ours(args):
     spec = workloads.spec_batched_fp32_1m(n=args.n, nq=args.nq * world)
     if rank == 0:
         W = workloads.build(spec, device=f"cuda:{local}", log=log)
+        tune_q, tune_gt = workloads.tuning_set(spec, W, device=f"cuda:{local}")
     barrier()
     if rank != 0:
         W = workloads.load(spec)
+        tune_q, tune_gt = workloads.tuning_set(spec, W)
     q_all, gt_all = W["queries"], W["gt"]
     qs = np.ascontiguousarray(q_all[shard(rank, args.nq)])
     gts = gt_all[shard(rank, args.nq)]
@@ -186,47 +198,57 @@ def bench_ours(args):
     handles[N.STORE_FP32] = handles[N.STORE_BF16]
     names = {N.STORE_FP32: "fp32", N.STORE_BF16: "bf16", N.STORE_FP8: "fp8"}
 
-    def run(L, M, store):
-        mode = N.MODE_NSG_SEQ if M == 1 else N.MODE_TOP_M
-        return handles[store].search(K=K, L=L, mode=mode, distance=N.DIST_NORM_IP, M=M, storage=store)
+    # The learned entry / L-budget network (trained on the GPU on held-out
+    # queries; rank 0 builds it, the others load the cached file).
+    model = None
+    if not args.no_learned:
+        if rank == 0:
+            model = workloads.learned_model(spec, handles[N.STORE_BF16], log=log)
+        barrier()
+        if rank != 0:
+            model = workloads.learned_model(spec, handles[N.STORE_BF16], log=None)
+    learned_opts = [dict(E=8, L_init=8, use_L=False), dict(E=32, L_init=0, use_L=False)]
 
-    # Operating points: per (storage, M) the smallest swept L reaching the
-    # recall target; per storage the fastest of those. Decided on rank 0.
-    sweep = []
-    best = {}
+    # Operating points, chosen by the autotuner on the tuning queries (not the
+    # evaluated ones) on rank 0: the plain FP32 search, and the fastest of all
+    # storages with and without the network.
+    Ms = [args.M] if args.M else M_SWEEP
     stores = [args.storage] if args.storage is not None else [N.STORE_FP32, N.STORE_BF16, N.STORE_FP8]
-    for store in stores:
-        for M in ([args.M] if args.M else M_SWEEP):
-            for L in ([args.L] if args.L else L_SWEEP):
-                run(L, M, store)
-                ids, st = run(L, M, store)
-                rec = recall(ids, gts, L, 100)
-                sweep.append({"storage": names[store], "M": M, "L": L, "recall100": round(rec, 5),
-                              "qps": round(nq / (st["kernel_ms"] / 1e3), 1)})
-                if rec >= RECALL_TARGET or (args.L and args.M):
-                    if store not in best or st["kernel_ms"] < best[store][0]:
-                        best[store] = (st["kernel_ms"], L, M)
-                    break
-    for store in stores:
-        best.setdefault(store, (1e30, L_SWEEP[-1], 1))
-    head_store = min(best, key=lambda k: best[k][0])
-    choice = [head_store, best[head_store][1], best[head_store][2]]
-    plain = [N.STORE_FP32, best.get(N.STORE_FP32, best[head_store])[1],
-             best.get(N.STORE_FP32, best[head_store])[2]]
-    both = ranks.broadcast_ints(choice + plain, 0)
-    choice, plain = both[:3], both[3:]
-    store, L, M = choice
+    choices = None
     if rank == 0:
-        log(f"operating point storage={names[store]} L={L} M={M}; plain fp32 L={plain[1]} M={plain[2]}; "
-            f"sweep {sweep}")
+        t0 = time.time()
+        plain = AT.tune(handles[N.STORE_FP32], tune_q, tune_gt, K=K, target=RECALL_TARGET,
+                        storages=(N.STORE_FP32,), Ms=Ms, wpbs=(2, 4))
+        cands = [plain]
+        for store in stores:
+            if store == N.STORE_FP32 and model is None:
+                continue
+            c = AT.tune(handles[store], tune_q, tune_gt, K=K, target=RECALL_TARGET, storages=(store,), Ms=Ms,
+                        wpbs=(2, 4), learned_model=model, learned_opts=learned_opts if model is not None else (),
+                        include_plain=store != N.STORE_FP32)
+            cands.append(c)
+        head = min(cands, key=lambda c: c.kernel_ms)
+        log(f"autotune {time.time() - t0:.1f}s: plain fp32 {plain.L}/{plain.M}/{plain.warps_per_block} "
+            f"{plain.kernel_ms:.3f} ms; head {names[head.storage]} L={head.L} M={head.M} "
+            f"w={head.warps_per_block} learned={head.learned} {head.kernel_ms:.3f} ms")
+        strip = lambda c: {k: v for k, v in c.__dict__.items() if k != "table"}
+        choices = {"plain": strip(plain), "head": strip(head),
+                   "tables": [r for c in cands for r in c.table]}
+    choices = ranks.broadcast_json(choices, 0)
+    plain = AT.Choice(**choices["plain"])
+    head = AT.Choice(**choices["head"])
+    if head.learned is not None:
+        LE.attach(handles[head.storage], model, **head.learned)
 
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
     sampler = ClockSampler(local)
 
-    def timed(cfg):
-        st_, L_, M_ = cfg
+    def run(c):
+        return handles[c.storage].search(K=K, distance=N.DIST_NORM_IP, **c.search_kwargs())
+
+    def timed(c):
         for _ in range(args.warmup):
-            run(L_, M_, st_)
+            run(c)
         barrier()
         torch.cuda.synchronize()
         kms = 0.0
@@ -235,7 +257,7 @@ def bench_ours(args):
         for _ in range(args.steps):
             flush.zero_()
             torch.cuda.synchronize()
-            ids_, st = run(L_, M_, st_)
+            ids_, st = run(c)
             kms += st["kernel_ms"]
             for k in tot_:
                 tot_[k] += st[k]
@@ -244,32 +266,65 @@ def bench_ours(args):
         return kms, tot_, ids_
 
     sampler.start()
-    kernel_ms, tot, last_ids = timed(choice)
+    kernel_ms, tot, last_ids = timed(head)
     kernel_ms_max = max_over_ranks(kernel_ms)
-    rec = recall(last_ids, gts, L, 100)
-    if (plain[1], plain[2]) == (L, M) and store == N.STORE_FP32:
-        p_ms, p_ids = kernel_ms, last_ids
+    rec = recall(last_ids, gts, 100, 100)
+    learned_info = None
+    if head.learned is not None:
+        Lq, fb, _ = LE.record(handles[head.storage], nq)
+        learned_info = {"options": head.learned, "fallback_rate": round(float(fb.mean()), 4),
+                        "mean_L": round(float(Lq.mean()), 1), "R": model.R,
+                        "training_queries": 200_000}
+    if (plain.storage, plain.L, plain.M, plain.learned, plain.warps_per_block) == (
+            head.storage, head.L, head.M, head.learned, head.warps_per_block):
+        p_ms, p_ids, p_tot = kernel_ms, last_ids, tot
     else:
-        p_ms, _, p_ids = timed(plain)
+        p_ms, p_tot, p_ids = timed(plain)
+        if head.learned is not None:  # timed(plain) ran without the flag; the network stays attached
+            pass
     p_ms_max = max_over_ranks(p_ms)
-    p_rec = recall(p_ids, gts, plain[1], 100)
+    p_rec = recall(p_ids, gts, 100, 100)
 
     # End to end through the host-pointer C ABI call.
-    mode = N.MODE_NSG_SEQ if M == 1 else N.MODE_TOP_M
-    ixh = handles[store]
+    ixh = handles[head.storage]
+    kw = head.search_kwargs()
     for _ in range(args.warmup):
-        ixh.search(qs, K=K, L=L, mode=mode, M=M, storage=store)
+        ixh.search(qs, K=K, **kw)
     barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(args.steps):
         flush.zero_()
         torch.cuda.synchronize()
-        ids_e2e, st_e2e = ixh.search(qs, K=K, L=L, mode=mode, M=M, storage=store)
+        ids_e2e, st_e2e = ixh.search(qs, K=K, **kw)
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     clocks = sampler.stop()
     assert np.array_equal(ids_e2e, last_ids)
+
+    # Batch sizes 1, 64 and 1000 through the asynchronous device-pointer entry
+    # point with the CUDA-graph-captured launch, batches back to back on one
+    # stream (device time from the first launch to the last result).
+    batching = {}
+    qd = torch.from_numpy(qs).cuda()
+    stream = torch.cuda.Stream()
+    for B, nb in ((1, 300), (64, 60), (1000, 10)):
+        outb = torch.empty((B, K), dtype=torch.int32, device="cuda")
+        kwb = dict(kw, flags=kw["flags"] | N.FLAG_CUDA_GRAPH)
+        for i in range(3):
+            ixh.search_device(qd[i * B:(i + 1) * B], outb, K=K, stream=stream, **kwb)
+        stream.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(nb):
+            s0 = (i * B) % (nq - B + 1)
+            ixh.search_device(qd[s0:s0 + B], outb, K=K, stream=stream, **kwb)
+        e1.record(stream)
+        stream.synchronize()
+        ms = e0.elapsed_time(e1)
+        batching[str(B)] = {"qps": round(nb * B / (ms / 1e3), 1), "ms_per_batch": round(ms / nb, 4)}
+    batching[str(nq)] = {"qps": round(nq * args.steps / (kernel_ms / 1e3), 1),
+                         "ms_per_batch": round(kernel_ms / args.steps, 4)}
 
     # Distance error of the returned ids against float64 (reduced storage re-ranks in float32).
     ids64 = last_ids[: min(200, nq)].astype(np.int64)
@@ -282,6 +337,7 @@ def bench_ours(args):
     # = n_dist * (s*d + 4 norm) + 4 * sum(1 + degree) over expansions + nq * (4d + 4K)
     #   (+ nq * L * (4d + 4) for the float32 re-rank of a reduced copy).
     steps = args.steps
+    store, L, M = head.storage, head.L, head.M
     s_el = {N.STORE_FP32: 4, N.STORE_BF16: 2, N.STORE_FP8: 1}[store]
     alg_bytes = (tot["n_dist"] * (s_el * d + 4) + 4 * tot["n_edges"]) / steps + nq * (4 * d + 4 * K)
     if store != N.STORE_FP32:
@@ -295,10 +351,12 @@ def bench_ours(args):
         try:
             with open(tp) as f:
                 tj = json.load(f)
-            if (tj.get("L"), tj.get("M"), tj.get("n"), tj.get("storage")) == (L, M, args.n, names[store]):
+            if (tj.get("L"), tj.get("M"), tj.get("n"), tj.get("storage"), tj.get("learned")) == (
+                    L, M, args.n, names[store], head.learned is not None):
                 traffic = tj["dram_bytes_per_query"] * nq
         except Exception:
             traffic = None
+    p_alg = (p_tot["n_dist"] * (4 * d + 4) + 4 * p_tot["n_edges"]) / steps + nq * (4 * d + 4 * K)
 
     total_q = nq * world * steps
     value = total_q / (kernel_ms_max / 1e3)
@@ -306,7 +364,7 @@ def bench_ours(args):
 
     cpu_base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu_base = cpu_baseline(W["paths"], L, nq, log)
+        cpu_base = cpu_baseline(W["paths"], plain.L, nq, log)
 
     if world > 1:
         dist.barrier()
@@ -319,26 +377,32 @@ def bench_ours(args):
             "config": {"workload": "batched search, 1M x 96d mixture64 (sigma 0.3, unit norm), "
                                    "NSG-style graph R=50, 10k queries per GPU, K=100",
                        "n": args.n, "d": d, "queries_per_gpu": nq, "K": K, "L": L, "M": M,
+                       "warps_per_block": head.warps_per_block,
                        "storage": names[store], "accumulate": "f32",
                        "rerank": "exact f32 of the final L" if store != N.STORE_FP32 else None,
+                       "learned": learned_info,
                        "mode": "NSG_SEQ" if M == 1 else "TOP_M", "distance": "NORM_IP",
                        "recall100": round(rec, 5), "recall_target": RECALL_TARGET,
                        "mean_rel_distance_error_vs_fp64": dist_err,
                        "avg_degree": round(W["meta"]["avg_degree"], 3), "width": W["meta"]["width"],
                        "parallelism": f"replicas x{world}",
+                       "operating_point": "autotuned on 10k held-out tuning queries (another seed); "
+                                          "recall and speed measured on the 10k evaluation queries",
                        "l2": "inputs larger than L2 (384 MB base) and a 256 MB L2 flush before each step",
-                       "sweep": sweep},
+                       "autotune": choices["tables"]},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
                          "peak_source": peak_kind,
                          "algorithmic_bytes_per_launch": int(alg_bytes)},
             "e2e": {"value": round(e2e_value, 1), "unit": UNIT,
-                    "h2d_bytes_per_step": nq * d * 4 + L * 4,
-                    "d2h_bytes_per_step": nq * K * 4 + nq * 16},
+                    "h2d_bytes_per_step": nq * d * 4,
+                    "d2h_bytes_per_step": nq * K * 4 + nq * 16 + 4},
             "gpu_launches": steps,
             "plain_fp32": {"value": round(nq * world * steps / (p_ms_max / 1e3), 1), "unit": UNIT,
-                           "L": plain[1], "M": plain[2], "recall100": round(p_rec, 5),
-                           "ms_per_step": round(p_ms_max / steps, 4)},
+                           "L": plain.L, "M": plain.M, "warps_per_block": plain.warps_per_block,
+                           "recall100": round(p_rec, 5), "ms_per_step": round(p_ms_max / steps, 4),
+                           "roofline_frac": round(p_alg / (p_ms / steps / 1e3) / 1e9 / peak, 4)},
+            "batching": batching,
             "counts_per_query": {k: round(v / steps / nq, 2) for k, v in tot.items()},
             "clocks": clocks,
             "cpu_baseline": cpu_base,
@@ -436,6 +500,7 @@ def main():
     ap.add_argument("--storage", type=int, default=None, choices=[0, 1, 2],
                     help="fix the storage (0 fp32, 1 bf16, 2 fp8; default: sweep)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="leave the learned entry network out")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

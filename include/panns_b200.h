@@ -73,7 +73,7 @@ typedef struct {
     uint32_t T;           /* PSS_V5: number of queues (workers + master, >= 1) */
     uint32_t L_local;     /* PSS_V5: worker queue capacity (0 = L) */
     uint32_t X;           /* PSS_V5: expansions per worker per stage (>= 1) */
-    uint32_t warps_per_block; /* 0 = autotuned */
+    uint32_t warps_per_block; /* warps (queries in flight) per block, <= 4; 0 = 4 */
     uint32_t storage;     /* panns_storage the search distances use: FP32 (exact), or
                              the reduced copy built by panns_set_base (NSG_SEQ / TOP_M
                              only; the final L are re-ranked in exact FP32) */
@@ -84,6 +84,8 @@ typedef struct {
                                 EFANNA: with the first L_query[i] of its L init ids. NULL = L
                                 for every query. No counterpart in the reference (one L per
                                 call, PSS.cpp:1218). */
+    uint32_t blocks_per_sm;  /* resident blocks per SM (0 = as many as fit); fewer leave more of
+                                the SM's L1 / shared array to L1, which caches gathered rows */
 } panns_search_params;
 
 /* Enqueue the launch (per-call memsets, query layout and the search kernel)

@@ -73,8 +73,9 @@ typedef struct {
     uint32_t E;           /* learned entries placed first in the queue (<= 64; 0 = none) */
     uint32_t L_init;      /* plain init ids after them (at most L_q - E; >= L fills the queue) */
     uint32_t L_min;       /* lower bound of the predicted queue length */
-    uint32_t use_L;       /* 1: queue length L_q = clamp(ceil(L_scale * exp(z_R)), max(K, L_min), L) */
+    uint32_t use_L;       /* 1: queue length L_q = clamp(ceil(L_scale * exp(L_exp * z_R)), max(K, L_min), L) */
     float L_scale;
+    float L_exp;          /* 1 = the regressor's L; < 1 narrows the spread of the budgets */
     float min_conf;       /* softmax confidence below which the query runs the plain search */
 } panns_learned_params;
 

@@ -112,7 +112,7 @@ def numeric_grad(params, X, cells, y, d, R, lam, idx, h=1e-6):
     return g
 
 
-def decide(params, X, d, R, reps, *, E, L_init, L_min, use_L, L_scale, min_conf, K, L):
+def decide(params, X, d, R, reps, *, E, L_init, L_min, use_L, L_scale, min_conf, K, L, L_exp=1.0):
     """The prologue's per-query decision: (fallback, L_q, entries, n_plain,
     confidence, regressor output, logits)."""
     _, _, Z, _ = forward(params, X, d, R, True)
@@ -123,7 +123,7 @@ def decide(params, X, d, R, reps, *, E, L_init, L_min, use_L, L_scale, min_conf,
         fb = not conf >= min_conf
         Lq = L
         if not fb and use_L:
-            v = L_scale * np.exp(z[R])
+            v = np.float32(L_scale) * np.exp(np.float32(L_exp) * z[R])
             lo = max(K, min(L_min, L))
             if v < L:
                 Lq = max(lo, int(np.ceil(max(v, 0.0))))

@@ -17,7 +17,7 @@
 // PANNS init list and the call's L, exactly the search without the network).
 // Otherwise the E representatives with the largest logits enter the queue
 // first, followed by at most L_init ids of the plain init list, and the
-// queue length is L_q = clamp(ceil(L_scale * exp(r)), max(K, L_min), L).
+// queue length is L_q = clamp(ceil(L_scale * exp(L_exp * r)), max(K, L_min), L).
 #pragma once
 
 #include <cuda_bf16.h>
@@ -41,7 +41,7 @@ struct MlpDev {
     const uint32_t *rep;      // R representative vertices (device ids)
     uint32_t d, R, E, L_init, L_min, use_entry, use_L;
     float min_conf;
-    float L_scale;
+    float L_scale, L_exp;     // L_q = L_scale * exp(L_exp * regressor)
     float *logits;            // warp slots x R scratch
     uint32_t *record;         // per query kMlpRecWords words (or null)
 };
@@ -154,7 +154,7 @@ static __device__ __noinline__ uint2 mlp_prologue(const MlpDev *__restrict__ mp,
     const bool fallback = !(conf >= mp->min_conf);
     uint32_t Lq = L;
     if (!fallback && mp->use_L) {
-        const float v = mp->L_scale * expf(r);
+        const float v = mp->L_scale * expf(mp->L_exp * r);
         const uint32_t lo = max(K, min(mp->L_min, L));
         if (v < (float) L) Lq = max(lo, (uint32_t) ceilf(fmaxf(v, 0.f)));
     }

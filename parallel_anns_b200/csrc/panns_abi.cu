@@ -690,6 +690,16 @@ int check_params(panns_index *h, const panns_search_params *p) {
 
 }  // namespace
 
+// Preferred shared-memory carveout (percent of the SM's 228 KB) for
+// `blocks` resident blocks of `smem` dynamic bytes each (1 KB reserved per
+// block); -1 (the driver's choice) when blocks is 0.
+static int carveout_percent(size_t smem, uint32_t blocks) {
+    if (!blocks) return -1;
+    const size_t need = (size_t) blocks * (smem + 1024);
+    const size_t total = 228u * 1024u;
+    return (int) std::min<size_t>(100, (need * 100 + total - 1) / total);
+}
+
 // What one search launch enqueues: two 4-byte memsets, the optional layout of
 // row-major device queries, and the kernel.
 struct LaunchDesc {
@@ -802,10 +812,24 @@ static int launch_search(panns_index *h, const panns_search_params *p, float *d_
     if (per_warp > (227u << 10))
         return fail(PANNS_EINVAL, "search: the queues (L, T x L_local) do not fit in shared memory");
     const size_t smem = (size_t) wpb * per_warp;
+    {
+        cudaFuncAttributes fa;
+        CU(cudaFuncGetAttributes(&fa, kern));
+        if ((int) (wpb * 32) > fa.maxThreadsPerBlock)
+            return fail(PANNS_EINVAL, "search: warps_per_block must be <= " + std::to_string(fa.maxThreadsPerBlock / 32) +
+                                          " for this kernel");
+    }
     CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+    // The L1 / shared-memory split: by default the driver's (enough shared
+    // memory for the most resident blocks); with blocks_per_sm, just enough
+    // shared memory for that many blocks, the rest of the array left to L1,
+    // which caches the gathered rows.
+    CU(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                            carveout_percent(smem, p->blocks_per_sm)));
     int per_sm = 0;
     CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (int) wpb * 32, smem));
     if (per_sm < 1) return fail(PANNS_EINVAL, "search: L too large for shared memory");
+    if (p->blocks_per_sm) per_sm = std::min(per_sm, (int) p->blocks_per_sm);
     uint32_t blocks = (uint32_t) per_sm * (uint32_t) h->num_sms;
     const uint32_t need_blocks = (nq + wpb - 1) / wpb;
     blocks = std::max(1u, std::min(blocks, need_blocks));
@@ -1328,7 +1352,15 @@ extern "C" int panns_search_static(panns_index *h, const panns_search_params *p,
     const uint32_t qcap = ((p->L + 31) / 32) * 32;
     const uint32_t wpb = p->warps_per_block ? p->warps_per_block : 4u;
     const size_t smem = (size_t) wpb * warp_smem_bytes(qcap);
+    {
+        cudaFuncAttributes fa;
+        CU(cudaFuncGetAttributes(&fa, kern));
+        if ((int) (wpb * 32) > fa.maxThreadsPerBlock)
+            return fail(PANNS_EINVAL, "search: warps_per_block must be <= " + std::to_string(fa.maxThreadsPerBlock / 32) +
+                                          " for this kernel");
+    }
     CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+    CU(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, -1));
     int per_sm = 0;
     CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (int) wpb * 32, smem));
     if (per_sm < 1) return fail(PANNS_EINVAL, "panns_search_static: L too large for shared memory");
@@ -1487,6 +1519,7 @@ extern "C" int panns_set_learned(panns_index *h, const float *params, uint32_t R
     m.use_L = lp->use_L;
     m.min_conf = lp->min_conf;
     m.L_scale = lp->L_scale;
+    m.L_exp = lp->L_exp;
     m.logits = h->mlp_logits.p;
     m.record = h->mlp_record.p;
     if (h->mlp_slots && h->mlp_logits.n < (size_t) h->mlp_slots * R) {  // R grew: re-size at the next launch

@@ -150,8 +150,8 @@ def forward(params, X, R, device=0):
 
 
 def attach(index, model: LearnedModel, *, E=16, L_init=1 << 30, L_min=0, use_L=True, L_scale=1.0,
-           min_conf=0.0):
-    lp = N.LearnedParams(E, min(L_init, 0xFFFFFFFF), L_min, 1 if use_L else 0, L_scale, min_conf)
+           L_exp=1.0, min_conf=0.0):
+    lp = N.LearnedParams(E, min(L_init, 0xFFFFFFFF), L_min, 1 if use_L else 0, L_scale, L_exp, min_conf)
     params = np.ascontiguousarray(model.params, dtype=np.float32)
     reps = np.ascontiguousarray(model.reps, dtype=np.uint32)
     N.check(N.load().panns_set_learned(index._h, N.ptr(params), model.R, N.ptr(reps), ctypes.byref(lp)))

@@ -47,7 +47,7 @@ FLAG_LEARNED = 2
 class SearchParams(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint32) for n in
                 ("mode", "distance", "K", "L", "M", "T", "L_local", "X", "warps_per_block", "storage",
-                 "flags")] + [("L_query", ctypes.c_void_p)]
+                 "flags")] + [("L_query", ctypes.c_void_p), ("blocks_per_sm", ctypes.c_uint32)]
 
 
 class MlpTrainParams(ctypes.Structure):
@@ -57,7 +57,7 @@ class MlpTrainParams(ctypes.Structure):
 
 class LearnedParams(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint32) for n in ("E", "L_init", "L_min", "use_L")] + [
-        (n, ctypes.c_float) for n in ("L_scale", "min_conf")]
+        (n, ctypes.c_float) for n in ("L_scale", "L_exp", "min_conf")]
 
 
 class Stats(ctypes.Structure):

@@ -48,3 +48,11 @@ class Ranks:
         t = torch.tensor(list(values), dtype=torch.int64, device=self.device)
         self._dist().broadcast(t, src)
         return [int(x) for x in t.tolist()]
+
+    def broadcast_json(self, obj, src: int = 0):
+        """A JSON-serialisable object from rank `src` to every rank."""
+        if self.world == 1:
+            return obj
+        box = [obj]
+        self._dist().broadcast_object_list(box, src)
+        return box[0]

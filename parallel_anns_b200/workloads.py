@@ -90,3 +90,32 @@ def load(spec):
     return {"base": fm.read_fvecs(p["base"]), "queries": fm.read_fvecs(p["query"]),
             "graph": fm.read_nsg(p["graph"]), "gt": fm.read_true_nn(p["truenn"])[0], "paths": p,
             "meta": meta}
+
+
+def tuning_set(spec, W, n_tune=10_000, device=None):
+    """Held-out queries (same mixture, another seed) with their float64 top-100,
+    for choosing operating points without looking at the evaluated queries."""
+    path = os.path.join(paths(spec)["root"], f"tune_q{n_tune}.npz")
+    if os.path.exists(path):
+        z = np.load(path)
+        return z["q"], z["gt"]
+    q = ds.gaussian_mixture(n_tune, spec["d"], spec["components"], spec["sigma"],
+                            seed=spec["query_seed"] + 1, means_seed=spec["base_seed"])
+    gt, _ = ground_truth(W["base"], W["graph"], q, spec["gt_k"], device)
+    np.savez(path, q=q, gt=gt)
+    return q, gt
+
+
+def learned_model(spec, index, n_train=200_000, R=1024, log=print):
+    """The entry / L-budget network for this workload, trained on n_train
+    held-out queries (cached next to the workload)."""
+    from . import learned as LE
+    cache = os.path.join(paths(spec)["root"], f"learned_R{R}_t{n_train}.npz")
+    train_q = ds.gaussian_mixture(n_train, spec["d"], spec["components"], spec["sigma"],
+                                  seed=spec["base_seed"] + 2000, means_seed=spec["base_seed"])
+    t0 = time.time()
+    m = LE.build_model(index, train_q, R=R, K=spec["gt_k"], M=8, L_ref=1000, T=10, epochs=10, batch=1024,
+                       lr=2e-3, lam=1.0, seed=0, kmeans_iters=15, cache=cache, log=log)
+    if log:
+        log(f"learned model ready in {time.time() - t0:.1f}s ({cache})")
+    return m

@@ -94,3 +94,30 @@ def test_single_query_batches(setup):
         ix.search_device(qd[i:i + 1], out[i:i + 1], K=100, L=128, flags=N.FLAG_CUDA_GRAPH)
     torch.cuda.synchronize()
     assert np.array_equal(out.cpu().numpy().view(np.uint32), ref)
+
+
+def test_warps_per_block_beyond_kernel_limit_rejected(setup):
+    ix, N, base, q, g = setup
+    with pytest.raises(N.PannsError) as e:
+        ix.search(K=10, L=64, warps_per_block=8)
+    assert e.value.code == -1
+    a, _ = ix.search(K=10, L=64, warps_per_block=2)
+    b, _ = ix.search(K=10, L=64, warps_per_block=1)
+    assert np.array_equal(a, b)
+    c, _ = ix.search(K=10, L=64, warps_per_block=4, blocks_per_sm=1)  # fewer resident blocks: same ids
+    assert np.array_equal(a, c)
+
+
+def test_autotuner_meets_target_on_tuning_queries(setup):
+    from parallel_anns_b200 import autotune as AT
+    from parallel_anns_b200.searching import ground_truth, recall
+    ix, N, base, q, g = setup
+    gt, _ = ground_truth(ix, q, 100)
+    c = AT.tune(ix, q, gt, K=100, target=0.97, Ms=(1, 4), wpbs=(2, 4), bpss=(0, 4), reps=1)
+    assert c.recall >= 0.97 and c.M in (1, 4) and c.warps_per_block in (2, 4)
+    ids, _ = ix.search(q, K=100, **c.search_kwargs())
+    assert recall(ids, gt, 100, 100) == pytest.approx(c.recall)
+    # every timed row reached the target; the choice is the fastest of them
+    rows = [r for r in c.table if r.get("L")]
+    assert all(r["recall"] >= 0.97 for r in rows)
+    assert c.kernel_ms == min(r["kernel_ms"] for r in rows)

@@ -102,7 +102,7 @@ def check_learned_search(ix, base, q, g, model, K, L, M, lp):
     dec = MO.decide(model.params, q, 96, model.R, model.reps, K=K, L=L, **{
         "E": lp["E"], "L_init": lp.get("L_init", 1 << 30), "L_min": lp.get("L_min", 0),
         "use_L": int(lp.get("use_L", True)), "L_scale": lp.get("L_scale", 1.0),
-        "min_conf": lp.get("min_conf", 0.0)})
+        "L_exp": lp.get("L_exp", 1.0), "min_conf": lp.get("min_conf", 0.0)})
     # decisions agree with the oracle (up to float32 near-ties)
     agree = 0
     for i, (ofb, oLq, oent, _, conf, r, lg) in enumerate(dec):
@@ -138,7 +138,7 @@ def test_learned_search_exact_given_decisions(small):
     p[-257:] += rng.normal(0, 0.5, 257).astype(np.float32)  # spread logits and the L output
     model = LE.LearnedModel(96, 256, p, reps)
     for lp, M in ((dict(E=16, L_init=1 << 30, use_L=True, L_scale=1.0), 4),
-                  (dict(E=8, L_init=24, use_L=True, L_scale=0.8, L_min=64), 1),
+                  (dict(E=8, L_init=24, use_L=True, L_scale=0.8, L_exp=0.6, L_min=64), 1),
                   (dict(E=40, L_init=0, use_L=False), 8)):
         check_learned_search(ix, base, q, g, model, 50, 200, M, lp)
 
