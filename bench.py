@@ -174,13 +174,16 @@ def bench_ours(args):
     max_over_ranks = ranks.max
 
     spec = workloads.spec_batched_fp32_1m(n=args.n, nq=args.nq * world)
+    fixed = bool(args.L and args.M)  # a given operating point: no tuning set, no autotuning
     if rank == 0:
         W = workloads.build(spec, device=f"cuda:{local}", log=log)
-        tune_q, tune_gt = workloads.tuning_set(spec, W, device=f"cuda:{local}")
+        if not fixed:
+            tune_q, tune_gt = workloads.tuning_set(spec, W, device=f"cuda:{local}")
     barrier()
     if rank != 0:
         W = workloads.load(spec)
-        tune_q, tune_gt = workloads.tuning_set(spec, W)
+        if not fixed:
+            tune_q, tune_gt = workloads.tuning_set(spec, W)
     q_all, gt_all = W["queries"], W["gt"]
     qs = np.ascontiguousarray(q_all[shard(rank, args.nq)])
     gts = gt_all[shard(rank, args.nq)]
@@ -201,7 +204,7 @@ def bench_ours(args):
     # The learned entry / L-budget network (trained on the GPU on held-out
     # queries; rank 0 builds it, the others load the cached file).
     model = None
-    if not args.no_learned:
+    if not args.no_learned and not fixed:
         if rank == 0:
             model = workloads.learned_model(spec, handles[N.STORE_BF16], log=log)
         barrier()
@@ -215,7 +218,11 @@ def bench_ours(args):
     Ms = [args.M] if args.M else M_SWEEP
     stores = [args.storage] if args.storage is not None else [N.STORE_FP32, N.STORE_BF16, N.STORE_FP8]
     choices = None
-    if rank == 0:
+    if fixed:
+        c = {"storage": args.storage or 0, "M": args.M, "L": args.L, "warps_per_block": args.wpb,
+             "learned": None, "blocks_per_sm": 0}
+        choices = {"plain": dict(c, storage=0), "head": c, "tables": []}
+    elif rank == 0:
         t0 = time.time()
         plain = AT.tune(handles[N.STORE_FP32], tune_q, tune_gt, K=K, target=RECALL_TARGET,
                         storages=(N.STORE_FP32,), Ms=Ms, wpbs=(2, 4))
@@ -386,8 +393,9 @@ def bench_ours(args):
                        "mean_rel_distance_error_vs_fp64": dist_err,
                        "avg_degree": round(W["meta"]["avg_degree"], 3), "width": W["meta"]["width"],
                        "parallelism": f"replicas x{world}",
-                       "operating_point": "autotuned on 10k held-out tuning queries (another seed); "
-                                          "recall and speed measured on the 10k evaluation queries",
+                       "operating_point": ("fixed by --L/--M" if fixed else
+                                           "autotuned on 10k held-out tuning queries (another seed); "
+                                           "recall and speed measured on the 10k evaluation queries"),
                        "l2": "inputs larger than L2 (384 MB base) and a 256 MB L2 flush before each step",
                        "autotune": choices["tables"]},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
@@ -501,6 +509,7 @@ def main():
                     help="fix the storage (0 fp32, 1 bf16, 2 fp8; default: sweep)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="leave the learned entry network out")
+    ap.add_argument("--wpb", type=int, default=2, help="warps per block with a fixed --L and --M")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -533,6 +533,27 @@ int kmeans_run(const float *rows, uint32_t n, uint32_t d, uint32_t k, uint32_t i
     return PANNS_OK;
 }
 
+int nearest_center(const float *rows, uint32_t n, uint32_t d, const uint32_t *center_rows, uint32_t k,
+                   uint32_t *cell, cudaStream_t s) {
+    Dev<float> cent, cn, G;
+    const uint32_t chunk = std::min<uint32_t>(n, 65536);
+    LCU(cent.alloc((size_t) k * d));
+    LCU(cn.alloc(k));
+    LCU(G.alloc((size_t) chunk * k));
+    gather_rows_kernel<<<k, 128, 0, s>>>(rows, d, center_rows, k, cent.p);
+    sqnorm_kernel<<<(k + 255) / 256, 256, 0, s>>>(cent.p, k, d, cn.p);
+    LCU(cudaGetLastError());
+    for (uint32_t r0 = 0; r0 < n; r0 += chunk) {
+        const uint32_t rows_c = std::min(chunk, n - r0);
+        LCU((gemm<float, float, false, true>(rows + (size_t) r0 * d, d, cent.p, d, G.p, k, rows_c, k, d, nullptr, 0,
+                                             s)));
+        argmin_kernel<<<(rows_c * 32 + 255) / 256, 256, 0, s>>>(G.p, rows_c, k, cn.p, cell + r0);
+        LCU(cudaGetLastError());
+    }
+    LCU(cudaStreamSynchronize(s));
+    return PANNS_OK;
+}
+
 namespace {
 __global__ void pack_kernel(const float *__restrict__ w, uint32_t d, uint32_t R, __nv_bfloat16 *__restrict__ wbf,
                             float *__restrict__ fb) {

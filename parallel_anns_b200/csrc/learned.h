@@ -22,6 +22,12 @@ int set_error(int code, const std::string &msg);
 int kmeans_run(const float *rows, uint32_t n, uint32_t d, uint32_t k, uint32_t iters, uint32_t seed,
                float *centroids, uint32_t *assign, uint32_t *rep, cudaStream_t stream);
 
+// cell[i] = the nearest (squared L2, via ||c||^2 - 2 x.c; ties to the lower
+// index) of the k rows center_rows[0..k) (device) for each of the n rows
+// (device, row-major, width d). Enqueued on `stream`, synchronised.
+int nearest_center(const float *rows, uint32_t n, uint32_t d, const uint32_t *center_rows, uint32_t k,
+                   uint32_t *cell, cudaStream_t stream);
+
 // Packs the float32 training parameters (layout of panns_mlp_param_count)
 // into the inference layout read by mlp_prologue: BF16 w1 (d x 256),
 // w2 (256 x 256), w3 (256 x R) into `wbf` (device, 256 (d + 256 + R)

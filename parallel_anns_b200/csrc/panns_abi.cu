@@ -67,42 +67,6 @@ __global__ void permute_rows_kernel(const float *__restrict__ raw, float *__rest
     }
 }
 
-// Locality order, step 1: the nearest of C pivot vertices for every vertex
-// (squared L2 on the raw rows; a layout heuristic, not part of the search
-// semantics). One warp per vertex, lanes stride over the pivots.
-__global__ void nearest_pivot_kernel(const float *__restrict__ raw, uint32_t n, int d,
-                                     const uint32_t *__restrict__ pivots, uint32_t C,
-                                     uint32_t *__restrict__ cell) {
-    const int lane = threadIdx.x & 31;
-    const uint64_t warps = (uint64_t) gridDim.x * (blockDim.x >> 5);
-    for (uint64_t v = blockIdx.x * (uint64_t) (blockDim.x >> 5) + (threadIdx.x >> 5); v < n;
-         v += warps) {
-        const float *x = raw + v * d;
-        float best = __int_as_float(0x7f800000);
-        uint32_t arg = 0;
-        for (uint32_t p = lane; p < C; p += 32) {
-            const float *y = raw + (uint64_t) pivots[p] * d;
-            float s = 0.f;
-            for (int j = 0; j < d; ++j) {
-                const float t = x[j] - y[j];
-                s = fmaf(t, t, s);
-            }
-            if (s < best) {
-                best = s;
-                arg = p;
-            }
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-            const float ob = __shfl_xor_sync(0xffffffffu, best, o);
-            const uint32_t oa = __shfl_xor_sync(0xffffffffu, arg, o);
-            if (ob < best || (ob == best && oa < arg)) {
-                best = ob;
-                arg = oa;
-            }
-        }
-        if (lane == 0) cell[v] = arg;
-    }
-}
 
 // ||v||^2 from the chain-major rows: lane c = FMA chain over its terms, then
 // the lanes summed 0..7 (core/Searching.202102022027.PSS_v5.dist_thresh.profiling.cpp:294-335).
@@ -434,9 +398,8 @@ static int finalize(panns_index *h) {
         CU(dpiv.ensure(C));
         CU(dcell.ensure(n));
         CU(cudaMemcpyAsync(dpiv.p, piv.data(), C * 4ull, cudaMemcpyHostToDevice, h->stream));
-        nearest_pivot_kernel<<<h->num_sms * 8, 256, 0, h->stream>>>(h->base_raw.p, n, (int) h->d, dpiv.p,
-                                                                    C, dcell.p);
-        CU(cudaGetLastError());
+        int rc = panns::nearest_center(h->base_raw.p, n, h->d, dpiv.p, C, dcell.p, h->stream);
+        if (rc) return rc;
         CU(cudaMemcpyAsync(cell.data(), dcell.p, n * 4ull, cudaMemcpyDeviceToHost, h->stream));
         CU(cudaStreamSynchronize(h->stream));
         std::vector<uint32_t> start(C + 1, 0);
