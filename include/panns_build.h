@@ -1,0 +1,56 @@
+/* panns_build — C ABI of the GPU graph construction of panns_b200.
+ *
+ * Builds the NSG-style proximity graph the search runs on: exact k-NN lists,
+ * relative-neighbourhood (MRNG) pruning to at most R neighbours, the medoid as
+ * entry vertex, and a reachability repair so that every vertex is reachable
+ * from the entry. It plays the part of efanna2e's IndexNSG::Build
+ * (include/efanna2e/index_nsg.cpp:638-718, whose pruning rule is
+ * sync_prune :233-283) on exact k-NN lists instead of search-based candidate
+ * pools, and IndexNSG::Save (:20-32) for the .nsg file.
+ *
+ * Semantics: d64(x, y) = one float64 FMA chain over the dimensions in order;
+ * knn(a) = the k vertices b != a with the smallest (d64(a, b), b); b in knn(a)
+ * is kept, in that order, unless a kept c has d64(c, b) < d64(a, b), up to R;
+ * entry = argmin over v of (d64(v, mean), v) with mean = the float64 mean of
+ * the rows; repair: every vertex not reachable from the entry, in id order,
+ * gets an in-edge from the first reachable vertex of its k-NN list (else from
+ * the entry). The k-NN lists come from a float32 screen of all pairs keeping
+ * k + 8 candidates per row, ranked exactly in float64.
+ */
+#ifndef PANNS_BUILD_H
+#define PANNS_BUILD_H
+
+#include "panns_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct panns_graph panns_graph;
+
+/* Build the graph of n row-major float32 vectors of width d (host pointer) on
+ * GPU `device`; knn_k <= 128, 0 < R <= knn_k. *out is released with
+ * panns_graph_free. */
+int panns_build_nsg(int device, const float *base, uint32_t n, uint32_t d, uint32_t knn_k, uint32_t R,
+                    panns_graph **out);
+
+/* Sizes of a built graph (each pointer optional): vertices, largest degree,
+ * entry vertex, total adjacency entries, in-edges added by the repair. */
+int panns_graph_info(const panns_graph *g, uint32_t *n, uint32_t *width, uint32_t *entry, uint64_t *n_edges,
+                     uint32_t *repaired);
+
+/* Copy out (each optional): offsets n + 1 (CSR), nbrs n_edges, knn n x knn_k. */
+int panns_graph_copy(const panns_graph *g, uint64_t *offsets, uint32_t *nbrs, uint32_t *knn);
+
+/* Write the graph as a .nsg file (uint32 width, uint32 entry, then per vertex
+ * uint32 degree and the ids), the layout IndexNSG::Save writes and
+ * panns_load_nsg / Searching::load_nsg_graph read. */
+int panns_graph_save_nsg(const panns_graph *g, const char *path);
+
+int panns_graph_free(panns_graph *g);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -59,6 +59,7 @@ def lib():
                                       ctypes.c_int, P, P, ctypes.c_int]
         L.po_search_top_m_lists.argtypes = [P, P, u32, u32, P, P, P, u32, P, u32, P, P, u32, u32,
                                             ctypes.c_int, P, P, ctypes.c_int]
+        L.po_build_nsg.argtypes = [P, u32, u32, u32, u32, P, P, P, P, ctypes.c_uint64, P, ctypes.c_int]
         L.po_search_pss.argtypes = [P, P, u32, u32, P, P, P, u32, P, u32, u32, u32, u32, u32,
                                     ctypes.c_int, P, P, ctypes.c_int]
         L.po_search_efanna.argtypes = [P, P, u32, u32, P, P, P, u32, P, u32, u32, ctypes.c_int,
@@ -280,3 +281,22 @@ def run_ref(name: str, out_path: str, env=None, **kw):
     K = int(kw.get("K", 100))
     ids = np.fromfile(out_path, dtype=np.uint32).reshape(-1, K)
     return ids, stats
+
+
+def build_nsg(base, k, R, threads=0):
+    """The graph construction restated in C: returns (NSGGraph, knn ids n x k)."""
+    from parallel_anns_b200.formats import NSGGraph
+    x = np.ascontiguousarray(base, dtype=np.float32)
+    n, d = x.shape
+    knn = np.empty((n, k), dtype=np.uint32)
+    off = np.empty(n + 1, dtype=np.uint64)
+    cap = n * R + n  # repair adds at most one in-edge per vertex
+    nbrs = np.empty(cap, dtype=np.uint32)
+    entry = np.zeros(1, dtype=np.uint32)
+    width = np.zeros(1, dtype=np.uint32)
+    rc = lib().po_build_nsg(_p(x), n, d, k, R, _p(knn), _p(entry), _p(off), _p(nbrs), cap, _p(width),
+                            _threads(threads))
+    if rc:
+        raise ValueError(f"po_build_nsg failed ({rc})")
+    g = NSGGraph(int(width[0]), int(entry[0]), off.astype(np.int64), nbrs[:int(off[-1])].copy())
+    return g, knn

@@ -728,3 +728,144 @@ int po_ground_truth_fp64(const float *data, uint32_t n, uint32_t d,
     }
     return err ? -2 : 0;
 }
+
+/* ---- graph construction (restates parallel_anns_b200/csrc/graph_build.cu) ----
+ * No PANNS counterpart: the graphs are built as BASELINE's configs describe
+ * (exact k-NN, MRNG prune, medoid, reachability repair); the pruning rule is
+ * efanna2e's sync_prune (include/efanna2e/index_nsg.cpp:233-283) on exact k-NN
+ * lists, the repair plays the part of its tree_grow (:638-718). */
+static double po_d64(const float *a, const float *b, uint32_t d) {
+    double acc = 0.0;
+    for (uint32_t j = 0; j < d; ++j) {
+        const double t = (double) a[j] - (double) b[j];
+        acc = fma(t, t, acc);
+    }
+    return acc;
+}
+
+typedef struct { double d; uint32_t id; } po_dk;
+
+static int po_dk_less(const po_dk *a, const po_dk *b) {
+    return a->d < b->d || (a->d == b->d && a->id < b->id);
+}
+
+int po_build_nsg(const float *x, uint32_t n, uint32_t d, uint32_t k, uint32_t R, uint32_t *knn_out,
+                 uint32_t *entry_out, uint64_t *off_out, uint32_t *nbrs_out, uint64_t nbrs_cap,
+                 uint32_t *width_out, int threads) {
+    if (n < 2 || k == 0 || k >= n || R == 0 || R > k) return -1;
+    uint32_t *pr = (uint32_t *) malloc((size_t) n * R * sizeof(uint32_t));
+    uint32_t *deg = (uint32_t *) calloc(n, sizeof(uint32_t));
+    double *kd = (double *) malloc((size_t) n * k * sizeof(double));
+    if (!pr || !deg || !kd) return -2;
+    /* exact k-NN by (d64, id) */
+#pragma omp parallel for num_threads(threads > 0 ? threads : 1) schedule(dynamic, 16)
+    for (uint32_t a = 0; a < n; ++a) {
+        po_dk *best = (po_dk *) malloc((size_t) (k + 1) * sizeof(po_dk));
+        uint32_t cnt = 0;
+        for (uint32_t b = 0; b < n; ++b) {
+            if (b == a) continue;
+            po_dk c = {po_d64(x + (size_t) a * d, x + (size_t) b * d, d), b};
+            if (cnt == k && !po_dk_less(&c, &best[k - 1])) continue;
+            uint32_t pos = cnt < k ? cnt : k - 1;
+            while (pos > 0 && po_dk_less(&c, &best[pos - 1])) {
+                best[pos] = best[pos - 1];
+                --pos;
+            }
+            best[pos] = c;
+            if (cnt < k) ++cnt;
+        }
+        for (uint32_t i = 0; i < k; ++i) {
+            knn_out[(size_t) a * k + i] = best[i].id;
+            kd[(size_t) a * k + i] = best[i].d;
+        }
+        free(best);
+        /* MRNG prune */
+        uint32_t nk = 0;
+        for (uint32_t i = 0; i < k && nk < R; ++i) {
+            const uint32_t b = knn_out[(size_t) a * k + i];
+            const double dab = kd[(size_t) a * k + i];
+            int occl = 0;
+            for (uint32_t c = 0; c < nk && !occl; ++c)
+                occl = po_d64(x + (size_t) pr[(size_t) a * R + c] * d, x + (size_t) b * d, d) < dab;
+            if (!occl) pr[(size_t) a * R + nk++] = b;
+        }
+        deg[a] = nk;
+    }
+    /* entry: nearest to the float64 mean (rows summed in id order) */
+    double *mean = (double *) calloc(d, sizeof(double));
+    for (uint32_t r = 0; r < n; ++r)
+        for (uint32_t j = 0; j < d; ++j) mean[j] += (double) x[(size_t) r * d + j];
+    for (uint32_t j = 0; j < d; ++j) mean[j] /= (double) n;
+    uint32_t entry = 0;
+    double be = 0.0;
+    for (uint32_t r = 0; r < n; ++r) {
+        double acc = 0.0;
+        for (uint32_t j = 0; j < d; ++j) {
+            const double t = (double) x[(size_t) r * d + j] - mean[j];
+            acc = fma(t, t, acc);
+        }
+        if (r == 0 || acc < be) {
+            be = acc;
+            entry = r;
+        }
+    }
+    free(mean);
+    /* adjacency with room for repair edges: lists as (start, length) in a growable pool */
+    uint32_t **lists = (uint32_t **) malloc(n * sizeof(uint32_t *));
+    uint32_t *len = (uint32_t *) malloc(n * sizeof(uint32_t));
+    uint32_t *cap = (uint32_t *) malloc(n * sizeof(uint32_t));
+    for (uint32_t a = 0; a < n; ++a) {
+        cap[a] = deg[a] + 4;
+        lists[a] = (uint32_t *) malloc(cap[a] * sizeof(uint32_t));
+        memcpy(lists[a], pr + (size_t) a * R, deg[a] * sizeof(uint32_t));
+        len[a] = deg[a];
+    }
+    uint8_t *reached = (uint8_t *) calloc(n, 1);
+    uint32_t *queue = (uint32_t *) malloc(n * sizeof(uint32_t));
+    /* BFS from src over not-yet-reached vertices */
+#define PO_WALK(src)                                                         \
+    do {                                                                     \
+        uint32_t qh = 0, qt = 0;                                             \
+        reached[src] = 1;                                                    \
+        queue[qt++] = (src);                                                 \
+        while (qh < qt) {                                                    \
+            const uint32_t v = queue[qh++];                                  \
+            for (uint32_t e = 0; e < len[v]; ++e) {                          \
+                const uint32_t w = lists[v][e];                              \
+                if (!reached[w]) { reached[w] = 1; queue[qt++] = w; }        \
+            }                                                                \
+        }                                                                    \
+    } while (0)
+    PO_WALK(entry);
+    for (uint32_t u = 0; u < n; ++u) {
+        if (reached[u]) continue;
+        uint32_t parent = entry;
+        for (uint32_t i = 0; i < k; ++i) {
+            const uint32_t c = knn_out[(size_t) u * k + i];
+            if (reached[c]) { parent = c; break; }
+        }
+        if (len[parent] == cap[parent]) {
+            cap[parent] *= 2;
+            lists[parent] = (uint32_t *) realloc(lists[parent], cap[parent] * sizeof(uint32_t));
+        }
+        lists[parent][len[parent]++] = u;
+        PO_WALK(u);
+    }
+#undef PO_WALK
+    uint64_t total = 0;
+    uint32_t width = 0;
+    off_out[0] = 0;
+    int err = 0;
+    for (uint32_t a = 0; a < n; ++a) {
+        if (total + len[a] > nbrs_cap) err = 1;
+        if (!err) memcpy(nbrs_out + total, lists[a], len[a] * sizeof(uint32_t));
+        total += len[a];
+        off_out[a + 1] = total;
+        if (len[a] > width) width = len[a];
+        free(lists[a]);
+    }
+    *entry_out = entry;
+    *width_out = width;
+    free(lists); free(len); free(cap); free(reached); free(queue); free(pr); free(deg); free(kd);
+    return err ? -3 : 0;
+}

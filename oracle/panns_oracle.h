@@ -90,6 +90,12 @@ int po_ground_truth_fp64(const float *data, uint32_t n, uint32_t d,
                          const float *queries, uint32_t nq, uint32_t k,
                          uint32_t *out_ids, double *out_dist, int threads);
 
+/* NSG-style graph: exact k-NN by float64 (one FMA chain per distance), MRNG
+ * prune to R, medoid entry, reachability repair (parallel_anns_b200/csrc/graph_build.cu). */
+int po_build_nsg(const float *x, uint32_t n, uint32_t d, uint32_t k, uint32_t R, uint32_t *knn_out,
+                 uint32_t *entry_out, uint64_t *off_out, uint32_t *nbrs_out, uint64_t nbrs_cap,
+                 uint32_t *width_out, int threads);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,438 @@
+// NSG-style graph construction on the GPU: exact k-NN lists, relative-
+// neighbourhood (MRNG) pruning to R, medoid entry, reachability repair.
+//
+// Semantics (restated by po_build_nsg in oracle/panns_oracle.c):
+//   * d64(x, y) = sum over j = 0..d-1, in order, of fma(t, t, acc) with
+//     t = (double) x_j - (double) y_j (one float64 chain).
+//   * knn(a) = the k vertices b != a with the smallest (d64(a, b), b).
+//   * prune(a): walk knn(a) in order; b is kept unless some already kept c has
+//     d64(c, b) < d64(a, b); at most R are kept (the NSG rule of
+//     include/efanna2e/index_nsg.cpp:233-283 applied to exact k-NN lists).
+//   * entry = the vertex with the smallest (d64(v, mean), v), mean = the float64
+//     mean of the rows summed in id order.
+//   * repair: from the entry, every vertex not reached (in id order) gets an
+//     in-edge from the first reached vertex of its k-NN list (else the entry),
+//     then everything it reaches is marked (index_nsg.cpp:638-718 plays this
+//     part with a DFS tree).
+// The k-NN search screens all pairs in float32 (||y||^2 - 2 x.y, tiled on
+// CUDA cores), keeps the C = k + 8 best per row, and ranks those by d64; the
+// result equals the exact k-NN unless a true neighbour falls outside the
+// float32 top C, which needs float32 rounding to move it past 8 others.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/panns_build.h"
+#include "learned.h"
+
+namespace panns {
+namespace {
+
+#define GCU(call)                                                                          \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess)                                                             \
+            return set_error(PANNS_ECUDA, std::string(#call ": ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+template <typename T>
+struct Buf {
+    T *p = nullptr;
+    ~Buf() {
+        if (p) cudaFree(p);
+    }
+    cudaError_t alloc(size_t n) { return cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)); }
+};
+
+constexpr int kBQ = 64;    // rows (queries) per block
+constexpr int kBV = 128;   // candidate rows per tile
+constexpr int kBK = 16;    // dimensions per shared-memory step
+constexpr int kMaxC = 136; // screen list length (k + 8 <= 136)
+
+__global__ void sqnorm32_kernel(const float *__restrict__ x, uint32_t n, uint32_t d, float *__restrict__ out) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    float s = 0.f;
+    for (uint32_t j = 0; j < d; ++j) s = fmaf(x[(size_t) r * d + j], x[(size_t) r * d + j], s);
+    out[r] = s;
+}
+
+// Float32 screen: for each of the kBQ rows of this block, the C candidates
+// (all rows but itself) with the smallest (||y||^2 - 2 x.y, id), over tiles of
+// kBV candidates. 256 threads: thread (ty, tx) computes a 4 x 8 block of the
+// 64 x 128 tile; then warp w inserts the tile into the lists of rows 8w..8w+7.
+__global__ void __launch_bounds__(256) screen_kernel(const float *__restrict__ x, uint32_t n, uint32_t d,
+                                                     const float *__restrict__ xn, uint32_t C,
+                                                     uint32_t *__restrict__ out_ids) {
+    extern __shared__ __align__(16) uint8_t sm[];
+    float *Qs = reinterpret_cast<float *>(sm);                 // [kBK][kBQ]
+    float *Vs = Qs + kBK * kBQ;                                // [kBK][kBV]
+    float *D = Vs + kBK * kBV;                                 // [kBQ][kBV + 1]
+    float *ld = D + kBQ * (kBV + 1);                           // [kBQ][C]
+    uint32_t *li = reinterpret_cast<uint32_t *>(ld + kBQ * C); // [kBQ][C]
+    uint32_t *cnt = li + kBQ * C;                              // [kBQ]
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t q0 = blockIdx.x * kBQ;
+    for (int i = tid; i < kBQ; i += 256) cnt[i] = 0;
+    const int ty = tid / 16, tx = tid % 16;  // rows ty*4.., cols tx*8..
+    __syncthreads();
+    for (uint32_t v0 = 0; v0 < n; v0 += kBV) {
+        float acc[4][8];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 8; ++j) acc[i][j] = 0.f;
+        for (uint32_t k0 = 0; k0 < d; k0 += kBK) {
+            for (int t = tid; t < kBK * kBQ; t += 256) {
+                const int kk = t % kBK, qq = t / kBK;
+                const uint32_t gq = q0 + qq, gk = k0 + kk;
+                Qs[kk * kBQ + qq] = (gq < n && gk < d) ? x[(size_t) gq * d + gk] : 0.f;
+            }
+            for (int t = tid; t < kBK * kBV; t += 256) {
+                const int kk = t % kBK, vv = t / kBK;
+                const uint32_t gv = v0 + vv, gk = k0 + kk;
+                Vs[kk * kBV + vv] = (gv < n && gk < d) ? x[(size_t) gv * d + gk] : 0.f;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int kk = 0; kk < kBK; ++kk) {
+                const float4 a4 = *reinterpret_cast<const float4 *>(Qs + kk * kBQ + ty * 4);
+                const float4 b4 = *reinterpret_cast<const float4 *>(Vs + kk * kBV + tx * 8);
+                const float4 b5 = *reinterpret_cast<const float4 *>(Vs + kk * kBV + tx * 8 + 4);
+                const float a[4] = {a4.x, a4.y, a4.z, a4.w};
+                const float b[8] = {b4.x, b4.y, b4.z, b4.w, b5.x, b5.y, b5.z, b5.w};
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+            }
+            __syncthreads();
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const uint32_t gq = q0 + ty * 4 + i;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const uint32_t gv = v0 + tx * 8 + j;
+                const bool ok = gv < n && gv != gq;
+                D[(ty * 4 + i) * (kBV + 1) + tx * 8 + j] =
+                    ok ? fmaf(-2.f, acc[i][j], xn[gv]) : __int_as_float(0x7f800000);
+            }
+        }
+        __syncthreads();
+        // Insert: rows 8w..8w+7 of this warp, each candidate that beats the
+        // row's current C-th (distance, id).
+        for (int r = warp * 8; r < warp * 8 + 8; ++r) {
+            float *rd = ld + r * C;
+            uint32_t *ri = li + r * C;
+            uint32_t c = cnt[r];
+            for (int j0 = 0; j0 < kBV; j0 += 32) {
+                const float dv = D[r * (kBV + 1) + j0 + lane];
+                const uint32_t iv = v0 + j0 + lane;
+                const float thr_d = c == C ? rd[C - 1] : __int_as_float(0x7f800000);
+                const uint32_t thr_i = c == C ? ri[C - 1] : 0xffffffffu;
+                bool want = dv < thr_d || (dv == thr_d && iv < thr_i);
+                want = want && !(dv == __int_as_float(0x7f800000));
+                uint32_t bm = __ballot_sync(0xffffffffu, want);
+                while (bm) {
+                    const int src = __ffs(bm) - 1;
+                    bm &= bm - 1;
+                    const float sd = __shfl_sync(0xffffffffu, dv, src);
+                    const uint32_t si = __shfl_sync(0xffffffffu, iv, src);
+                    // still better than the C-th after earlier inserts?
+                    if (c == C && !(sd < rd[C - 1] || (sd == rd[C - 1] && si < ri[C - 1]))) continue;
+                    // position = number of entries smaller than (sd, si)
+                    uint32_t pos = 0;
+                    for (uint32_t e0 = 0; e0 < c; e0 += 32) {
+                        const uint32_t e = e0 + lane;
+                        const bool less = e < c && (rd[e] < sd || (rd[e] == sd && ri[e] < si));
+                        pos += __popc(__ballot_sync(0xffffffffu, less));
+                    }
+                    const uint32_t end = c < C ? c : C - 1;  // last index that moves
+                    // shift [pos, end) up by one, from the top down in chunks of 32
+                    for (int e0 = (int) end - 1; e0 >= (int) pos; e0 -= 32) {
+                        const int e = e0 - lane;
+                        float td = 0.f;
+                        uint32_t ti = 0;
+                        const bool mv = e >= (int) pos;
+                        if (mv) {
+                            td = rd[e];
+                            ti = ri[e];
+                        }
+                        __syncwarp();
+                        if (mv) {
+                            rd[e + 1] = td;
+                            ri[e + 1] = ti;
+                        }
+                        __syncwarp();
+                    }
+                    if (lane == 0) {
+                        rd[pos] = sd;
+                        ri[pos] = si;
+                    }
+                    __syncwarp();
+                    if (c < C) ++c;
+                }
+            }
+            if (lane == 0) cnt[r] = c;
+            __syncwarp();
+        }
+        __syncthreads();
+    }
+    for (int r = warp; r < kBQ; r += 8) {
+        const uint32_t gq = q0 + r;
+        if (gq >= n) continue;
+        for (uint32_t e = lane; e < C; e += 32)
+            out_ids[(size_t) gq * C + e] = e < cnt[r] ? li[r * C + e] : 0xffffffffu;
+    }
+}
+
+__device__ __forceinline__ double d64(const float *__restrict__ a, const float *__restrict__ b, uint32_t d) {
+    double acc = 0.0;
+    for (uint32_t j = 0; j < d; ++j) {
+        const double t = (double) a[j] - (double) b[j];
+        acc = fma(t, t, acc);
+    }
+    return acc;
+}
+
+// One warp per row: float64 distances of its C screened candidates, ranked by
+// (d64, id); the k best go out (ids and distances).
+__global__ void rerank_kernel(const float *__restrict__ x, uint32_t n, uint32_t d, const uint32_t *__restrict__ cand,
+                              uint32_t C, uint32_t k, uint32_t *__restrict__ knn, double *__restrict__ knn_d) {
+    __shared__ double sd[8][kMaxC];
+    __shared__ uint32_t si[8][kMaxC];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t a = blockIdx.x * 8 + w;
+    if (a >= n) return;
+    const float *xa = x + (size_t) a * d;
+    for (uint32_t e = lane; e < C; e += 32) {
+        const uint32_t b = cand[(size_t) a * C + e];
+        si[w][e] = b;
+        sd[w][e] = b < n ? d64(xa, x + (size_t) b * d, d) : __longlong_as_double(0x7ff0000000000000ll);
+    }
+    __syncwarp();
+    for (uint32_t e = lane; e < C; e += 32) {
+        const double de = sd[w][e];
+        const uint32_t ie = si[w][e];
+        uint32_t rank = 0;
+        for (uint32_t f = 0; f < C; ++f) {
+            const double df = sd[w][f];
+            const uint32_t jf = si[w][f];
+            rank += (df < de || (df == de && jf < ie)) ? 1u : 0u;
+        }
+        if (rank < k) {
+            knn[(size_t) a * k + rank] = ie;
+            knn_d[(size_t) a * k + rank] = de;
+        }
+    }
+}
+
+// One warp per row: MRNG pruning of its k-NN list to at most R.
+__global__ void prune_kernel(const float *__restrict__ x, uint32_t n, uint32_t d, const uint32_t *__restrict__ knn,
+                             const double *__restrict__ knn_d, uint32_t k, uint32_t R, uint32_t *__restrict__ out,
+                             uint32_t *__restrict__ deg) {
+    extern __shared__ uint32_t kept_all[];  // [8][R]
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t a = blockIdx.x * 8 + w;
+    if (a >= n) return;
+    uint32_t *kept = kept_all + w * R;
+    uint32_t nk = 0;
+    for (uint32_t i = 0; i < k && nk < R; ++i) {
+        const uint32_t b = knn[(size_t) a * k + i];
+        if (b >= n) break;
+        const double dab = knn_d[(size_t) a * k + i];
+        const float *xb = x + (size_t) b * d;
+        bool occl = false;
+        for (uint32_t c0 = 0; c0 < nk && !occl; c0 += 32) {
+            const uint32_t c = c0 + lane;
+            const bool o = c < nk && d64(x + (size_t) kept[c] * d, xb, d) < dab;
+            occl = __any_sync(0xffffffffu, o);
+        }
+        if (!occl) {
+            if (lane == 0) kept[nk] = b;
+            __syncwarp();
+            ++nk;
+        }
+    }
+    for (uint32_t e = lane; e < nk; e += 32) out[(size_t) a * R + e] = kept[e];
+    if (lane == 0) deg[a] = nk;
+}
+
+// d64 of every row to one float64 point (the mean).
+__global__ void dist_to_point_kernel(const float *__restrict__ x, uint32_t n, uint32_t d,
+                                     const double *__restrict__ p, double *__restrict__ out) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    double acc = 0.0;
+    for (uint32_t j = 0; j < d; ++j) {
+        const double t = (double) x[(size_t) r * d + j] - p[j];
+        acc = fma(t, t, acc);
+    }
+    out[r] = acc;
+}
+
+}  // namespace
+}  // namespace panns
+
+struct panns_graph {
+    uint32_t n = 0, width = 0, entry = 0;
+    std::vector<uint64_t> off;
+    std::vector<uint32_t> nbrs;
+    std::vector<uint32_t> knn;  // n x k (kept for the repair and for callers)
+    uint32_t k = 0;
+    uint32_t repaired = 0;
+};
+
+using namespace panns;
+
+extern "C" {
+
+int panns_build_nsg(int device, const float *base, uint32_t n, uint32_t d, uint32_t knn_k, uint32_t R,
+                    panns_graph **out) {
+    if (!out || !base) return set_error(PANNS_EINVAL, "panns_build_nsg: NULL argument");
+    *out = nullptr;
+    if (n < 2 || d == 0) return set_error(PANNS_EINVAL, "panns_build_nsg: need n >= 2, d > 0");
+    if (knn_k == 0 || knn_k >= n) return set_error(PANNS_EINVAL, "panns_build_nsg: need 0 < knn_k < n");
+    if (knn_k + 8 > (uint32_t) kMaxC) return set_error(PANNS_EINVAL, "panns_build_nsg: knn_k > 128 is not supported");
+    if (R == 0 || R > knn_k) return set_error(PANNS_EINVAL, "panns_build_nsg: need 0 < R <= knn_k");
+    const uint32_t k = knn_k, C = std::min(knn_k + 8, n - 1);
+    GCU(cudaSetDevice(device));
+    cudaStream_t s = nullptr;
+    GCU(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    struct SG {
+        cudaStream_t s;
+        ~SG() { cudaStreamDestroy(s); }
+    } sg{s};
+    Buf<float> x, xn;
+    Buf<uint32_t> cand, knn, pr, deg;
+    Buf<double> knn_d, mean, dm;
+    GCU(x.alloc((size_t) n * d));
+    GCU(xn.alloc(n));
+    GCU(cand.alloc((size_t) n * C));
+    GCU(knn.alloc((size_t) n * k));
+    GCU(knn_d.alloc((size_t) n * k));
+    GCU(pr.alloc((size_t) n * R));
+    GCU(deg.alloc(n));
+    GCU(mean.alloc(d));
+    GCU(dm.alloc(n));
+    GCU(cudaMemcpyAsync(x.p, base, (size_t) n * d * 4, cudaMemcpyHostToDevice, s));
+    sqnorm32_kernel<<<(n + 255) / 256, 256, 0, s>>>(x.p, n, d, xn.p);
+    const size_t smem = (size_t) (kBK * kBQ + kBK * kBV + kBQ * (kBV + 1)) * 4 + (size_t) kBQ * C * 8 + kBQ * 4;
+    GCU(cudaFuncSetAttribute(screen_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+    screen_kernel<<<(n + kBQ - 1) / kBQ, 256, smem, s>>>(x.p, n, d, xn.p, C, cand.p);
+    GCU(cudaGetLastError());
+    rerank_kernel<<<(n + 7) / 8, 256, 0, s>>>(x.p, n, d, cand.p, C, k, knn.p, knn_d.p);
+    GCU(cudaGetLastError());
+    prune_kernel<<<(n + 7) / 8, 256, 8 * R * 4, s>>>(x.p, n, d, knn.p, knn_d.p, k, R, pr.p, deg.p);
+    GCU(cudaGetLastError());
+    // Entry: float64 mean of the rows in id order (host), then the nearest row.
+    std::vector<double> mh(d, 0.0);
+    for (uint32_t r = 0; r < n; ++r)
+        for (uint32_t j = 0; j < d; ++j) mh[j] += (double) base[(size_t) r * d + j];
+    for (uint32_t j = 0; j < d; ++j) mh[j] /= (double) n;
+    GCU(cudaMemcpyAsync(mean.p, mh.data(), d * 8ull, cudaMemcpyHostToDevice, s));
+    dist_to_point_kernel<<<(n + 255) / 256, 256, 0, s>>>(x.p, n, d, mean.p, dm.p);
+    GCU(cudaGetLastError());
+    std::unique_ptr<panns_graph> g(new panns_graph());
+    g->n = n;
+    g->k = k;
+    std::vector<uint32_t> prh((size_t) n * R), degh(n);
+    std::vector<double> dmh(n);
+    g->knn.resize((size_t) n * k);
+    GCU(cudaMemcpyAsync(prh.data(), pr.p, prh.size() * 4, cudaMemcpyDeviceToHost, s));
+    GCU(cudaMemcpyAsync(degh.data(), deg.p, n * 4ull, cudaMemcpyDeviceToHost, s));
+    GCU(cudaMemcpyAsync(dmh.data(), dm.p, n * 8ull, cudaMemcpyDeviceToHost, s));
+    GCU(cudaMemcpyAsync(g->knn.data(), knn.p, g->knn.size() * 4, cudaMemcpyDeviceToHost, s));
+    GCU(cudaStreamSynchronize(s));
+    uint32_t entry = 0;
+    for (uint32_t r = 1; r < n; ++r)
+        if (dmh[r] < dmh[entry]) entry = r;
+    g->entry = entry;
+    // Adjacency lists, then the reachability repair from the entry.
+    std::vector<std::vector<uint32_t>> lists(n);
+    for (uint32_t a = 0; a < n; ++a) lists[a].assign(prh.begin() + (size_t) a * R, prh.begin() + (size_t) a * R + degh[a]);
+    std::vector<uint8_t> reached(n, 0);
+    std::deque<uint32_t> dq;
+    auto walk = [&](uint32_t src) {
+        reached[src] = 1;
+        dq.push_back(src);
+        while (!dq.empty()) {
+            const uint32_t v = dq.front();
+            dq.pop_front();
+            for (uint32_t w : lists[v])
+                if (!reached[w]) {
+                    reached[w] = 1;
+                    dq.push_back(w);
+                }
+        }
+    };
+    walk(entry);
+    for (uint32_t u = 0; u < n; ++u) {
+        if (reached[u]) continue;
+        uint32_t parent = entry;
+        for (uint32_t i = 0; i < k; ++i) {
+            const uint32_t c = g->knn[(size_t) u * k + i];
+            if (c < n && reached[c]) {
+                parent = c;
+                break;
+            }
+        }
+        lists[parent].push_back(u);
+        ++g->repaired;
+        walk(u);
+    }
+    g->off.assign(n + 1, 0);
+    for (uint32_t a = 0; a < n; ++a) {
+        g->off[a + 1] = g->off[a] + lists[a].size();
+        g->width = std::max<uint32_t>(g->width, (uint32_t) lists[a].size());
+    }
+    g->nbrs.resize(g->off[n]);
+    for (uint32_t a = 0; a < n; ++a) std::copy(lists[a].begin(), lists[a].end(), g->nbrs.begin() + g->off[a]);
+    *out = g.release();
+    return PANNS_OK;
+}
+
+int panns_graph_info(const panns_graph *g, uint32_t *n, uint32_t *width, uint32_t *entry, uint64_t *n_edges,
+                     uint32_t *repaired) {
+    if (!g) return set_error(PANNS_EINVAL, "panns_graph_info: NULL graph");
+    if (n) *n = g->n;
+    if (width) *width = g->width;
+    if (entry) *entry = g->entry;
+    if (n_edges) *n_edges = g->off.empty() ? 0 : g->off.back();
+    if (repaired) *repaired = g->repaired;
+    return PANNS_OK;
+}
+
+int panns_graph_copy(const panns_graph *g, uint64_t *offsets, uint32_t *nbrs, uint32_t *knn) {
+    if (!g) return set_error(PANNS_EINVAL, "panns_graph_copy: NULL graph");
+    if (offsets) memcpy(offsets, g->off.data(), g->off.size() * 8);
+    if (nbrs && !g->nbrs.empty()) memcpy(nbrs, g->nbrs.data(), g->nbrs.size() * 4);
+    if (knn) memcpy(knn, g->knn.data(), g->knn.size() * 4);
+    return PANNS_OK;
+}
+
+int panns_graph_save_nsg(const panns_graph *g, const char *path) {
+    if (!g || !path) return set_error(PANNS_EINVAL, "panns_graph_save_nsg: NULL argument");
+    FILE *f = fopen(path, "wb");
+    if (!f) return set_error(PANNS_EIO, std::string("panns_graph_save_nsg: cannot open ") + path);
+    bool ok = fwrite(&g->width, 4, 1, f) == 1 && fwrite(&g->entry, 4, 1, f) == 1;
+    for (uint32_t a = 0; ok && a < g->n; ++a) {
+        const uint32_t k = (uint32_t) (g->off[a + 1] - g->off[a]);
+        ok = fwrite(&k, 4, 1, f) == 1 && (k == 0 || fwrite(g->nbrs.data() + g->off[a], 4, k, f) == k);
+    }
+    ok = (fclose(f) == 0) && ok;
+    return ok ? PANNS_OK : set_error(PANNS_EIO, std::string("panns_graph_save_nsg: write failed: ") + path);
+}
+
+int panns_graph_free(panns_graph *g) {
+    delete g;
+    return PANNS_OK;
+}
+
+}  // extern "C"

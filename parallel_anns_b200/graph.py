@@ -1,0 +1,46 @@
+"""GPU graph construction (include/panns_build.h): exact k-NN, MRNG prune to
+R, medoid entry, reachability repair — the NSG-style graphs the benchmark
+workloads describe, built by the library's own kernels."""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import native as N
+from .formats import NSGGraph
+
+
+def build_nsg(base: np.ndarray, R: int = 50, knn_k: int = 64, device: int = 0, with_knn: bool = False):
+    """Build the graph of ``base`` (n x d float32) on GPU ``device``.
+    Returns an NSGGraph (and the n x knn_k k-NN ids if ``with_knn``)."""
+    x = np.ascontiguousarray(base, dtype=np.float32)
+    n, d = x.shape
+    lib = N.load()
+    g = ctypes.c_void_p()
+    N.check(lib.panns_build_nsg(device, N.ptr(x), n, d, knn_k, R, ctypes.byref(g)))
+    try:
+        vals = [ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint64(), ctypes.c_uint32()]
+        N.check(lib.panns_graph_info(g, *[ctypes.byref(v) for v in vals]))
+        _, width, entry, n_edges, repaired = [v.value for v in vals]
+        off = np.empty(n + 1, dtype=np.uint64)
+        nbrs = np.empty(max(n_edges, 1), dtype=np.uint32)
+        knn = np.empty((n, knn_k), dtype=np.uint32) if with_knn else None
+        N.check(lib.panns_graph_copy(g, N.ptr(off), N.ptr(nbrs), N.ptr(knn) if with_knn else None))
+    finally:
+        lib.panns_graph_free(g)
+    graph = NSGGraph(int(width), int(entry), off.astype(np.int64), nbrs[:n_edges].copy())
+    graph.repaired = repaired
+    return (graph, knn) if with_knn else graph
+
+
+def save_nsg_gpu_built(base: np.ndarray, path: str, R: int = 50, knn_k: int = 64, device: int = 0) -> None:
+    """Build and write the .nsg file directly from the library (IndexNSG::Save layout)."""
+    x = np.ascontiguousarray(base, dtype=np.float32)
+    lib = N.load()
+    g = ctypes.c_void_p()
+    N.check(lib.panns_build_nsg(device, N.ptr(x), x.shape[0], x.shape[1], knn_k, R, ctypes.byref(g)))
+    try:
+        N.check(lib.panns_graph_save_nsg(g, path.encode()))
+    finally:
+        lib.panns_graph_free(g)

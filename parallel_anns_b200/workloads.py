@@ -2,9 +2,9 @@
 
 ``batched_fp32_1m``: N = 1,000,000 base vectors, d = 96, from a 64-component
 isotropic Gaussian mixture (means ~ N(0, 1), sigma = 0.3), L2-normalised;
-queries from the same mixture; NSG-style graph with R = 50 built by
-``datasets.build_nsg_graph`` (exact 64-NN, MRNG prune, medoid entry,
-reachability repair); ground truth = top-100 by float64 brute force.
+queries from the same mixture; NSG-style graph with R = 50 (exact 64-NN,
+MRNG prune, medoid entry, reachability repair) built on the GPU by
+``graph.build_nsg``; ground truth = top-100 by float64 brute force.
 
 Ground truth: top-100 by float64 brute force (``panns_ground_truth`` on the GPU).
 Files are written in the reference's formats (fvecs, .nsg, true-NN) to a cache
@@ -53,7 +53,7 @@ def build(spec, device=None, log=print):
     q = ds.gaussian_mixture(spec["nq"], spec["d"], spec["components"], spec["sigma"],
                             seed=spec["query_seed"], means_seed=spec["base_seed"])
     t1 = time.time()
-    g = ds.build_nsg_graph(base, R=spec["R"], knn_k=spec["knn_k"], device=device)
+    g = build_graph(base, spec, device)
     t2 = time.time()
     gt_ids, gt_d = ground_truth(base, g, q, spec["gt_k"], device)
     t3 = time.time()
@@ -67,6 +67,17 @@ def build(spec, device=None, log=print):
         json.dump(meta, f)
     log(f"workload {spec['name']}: built in {time.time() - t0:.1f}s {meta['build_s']}")
     return {"base": base, "queries": q, "graph": g, "gt": gt_ids, "paths": p, "meta": meta}
+
+
+def build_graph(base, spec, device=None):
+    """The workload's graph: the library's GPU construction (include/panns_build.h)
+    when a GPU is present, else the torch restatement in datasets.py (same rule)."""
+    import torch
+    if torch.cuda.is_available():
+        from .graph import build_nsg
+        dev = torch.device(device) if device is not None else torch.device("cuda", 0)
+        return build_nsg(base, R=spec["R"], knn_k=spec["knn_k"], device=dev.index or 0)
+    return ds.build_nsg_graph(base, R=spec["R"], knn_k=spec["knn_k"], device="cpu")
 
 
 def ground_truth(base, graph, queries, k, device=None):

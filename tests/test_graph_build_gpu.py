@@ -1,0 +1,79 @@
+"""GPU graph construction (include/panns_build.h) against the C oracle
+(po_build_nsg, pinned by tests/test_graph_oracle.py): identical k-NN lists,
+adjacency, entry vertex and width, on mixtures at d = 96 and d = 24, on data
+with duplicated rows (ties by id) and with far clusters (repairs); the .nsg
+written by the library reads back to the same graph and every vertex is
+reachable from the entry."""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def same_graph(g, h):
+    return (g.entry == h.entry and g.width == h.width and np.array_equal(g.offsets, h.offsets)
+            and np.array_equal(g.nbrs, h.nbrs))
+
+
+@pytest.mark.parametrize("n,d,k,R,seed", [(6000, 96, 64, 50, 1), (3000, 24, 32, 24, 2), (1500, 128, 40, 20, 3)])
+def test_gpu_graph_equals_oracle(n, d, k, R, seed):
+    from parallel_anns_b200 import datasets as ds
+    from parallel_anns_b200.graph import build_nsg
+    x = ds.gaussian_mixture(n, d, seed=seed, means_seed=seed)
+    g, knn = build_nsg(x, R=R, knn_k=k, with_knn=True)
+    og, oknn = O.build_nsg(x, k, R)
+    bad = np.nonzero((knn != oknn).any(1))[0]
+    assert bad.size == 0, f"k-NN rows differ: {bad[:10]}"
+    assert same_graph(g, og)
+
+
+def test_gpu_graph_ties_and_repairs():
+    from parallel_anns_b200.graph import build_nsg
+    rng = np.random.default_rng(9)
+    a = rng.standard_normal((700, 32)).astype(np.float32)
+    x = np.concatenate([a, a[:200], a[:40] + 40.0, a[:3] - 80.0]).astype(np.float32)
+    g, knn = build_nsg(x, R=8, knn_k=16, with_knn=True)
+    og, oknn = O.build_nsg(x, 16, 8)
+    assert np.array_equal(knn, oknn)
+    assert same_graph(g, og)
+    assert g.repaired > 0
+
+
+def test_gpu_graph_file_and_reachability():
+    from parallel_anns_b200 import datasets as ds
+    from parallel_anns_b200 import formats as fm
+    from parallel_anns_b200.graph import build_nsg, save_nsg_gpu_built
+    x = ds.gaussian_mixture(4000, 96, seed=4, means_seed=4)
+    g = build_nsg(x, R=32, knn_k=48)
+    with tempfile.TemporaryDirectory() as t:
+        p = os.path.join(t, "g.nsg")
+        save_nsg_gpu_built(x, p, R=32, knn_k=48)
+        h = fm.read_nsg(p)
+    assert same_graph(g, h)
+    seen = np.zeros(g.n, bool)
+    stack = [g.entry]
+    seen[g.entry] = True
+    while stack:
+        v = stack.pop()
+        for w in g.neighbors(v):
+            if not seen[w]:
+                seen[w] = True
+                stack.append(int(w))
+    assert seen.all()
+
+
+def test_gpu_graph_errors():
+    from parallel_anns_b200 import native as N
+    from parallel_anns_b200.graph import build_nsg
+    x = np.zeros((10, 8), np.float32)
+    with pytest.raises(N.PannsError):
+        build_nsg(x, R=4, knn_k=10)  # k must be < n
+    with pytest.raises(N.PannsError):
+        build_nsg(x, R=6, knn_k=5)   # R <= k
+    with pytest.raises(N.PannsError):
+        build_nsg(np.zeros((300, 8), np.float32), R=4, knn_k=200)  # k <= 128
