@@ -16,6 +16,11 @@
 //   -DREF_TOPM    core/Searching.202011241533.top_m_pure.cpp
 //                 (seq_search_simple_search :1486-1605, seq_search_with_top_m_pure
 //                  :1382-1484, para_search_with_top_m_pure :1881-2070)
+//   -DREF_MULTI   core/Searching.202107292234.PSS_v5.multi_queries.LG.cpp
+//                 (para_search_PSS_v5_multi_queries_LG :1379; inter-query mode: an
+//                  outer OpenMP loop over queries, T / inner threads, each query
+//                  searched by `inner` PSS_v5 threads, as in
+//                  app/PSS_v5_multi_queries_LG.cpp:89-160)
 //   -DREF_EFANNA  include/efanna2e/index_nsg.cpp (Search :452-518,
 //                 SearchWithOptGraph :520-611; call sequence of
 //                 app/profile_find_L_seq_single_query_simple_search.cpp:144-171)
@@ -33,6 +38,7 @@
 // best repetition), qps, recall100 (if truenn=), rep_times (every repetition,
 // timed like app/PSS_v5_distance_threshold_profiling.cpp:129-152: a
 // std::chrono bracket around prepare_init_ids and the query loop).
+#include <algorithm>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -49,10 +55,12 @@
 #include "core/Searching.202102031939.PSS_v5.large_graph.dist_thresh.profiling.h"
 #elif defined(REF_TOPM)
 #include "core/Searching.202011241533.top_m_pure.h"
+#elif defined(REF_MULTI)
+#include "core/Searching.202107292234.PSS_v5.multi_queries.LG.h"
 #elif defined(REF_EFANNA)
 #include "include/efanna2e/index_nsg.h"
 #else
-#error "define one of REF_PSS REF_PSS_LG REF_TOPM REF_EFANNA"
+#error "define one of REF_PSS REF_PSS_LG REF_TOPM REF_MULTI REF_EFANNA"
 #endif
 
 static std::map<std::string, std::string> g_args;
@@ -134,7 +142,48 @@ int main(int argc, char **argv) {
     const unsigned reps = arg_u("reps", "1");
     const std::string mode = arg_s("mode", "");
 
-#if defined(REF_PSS) || defined(REF_PSS_LG) || defined(REF_TOPM)
+#if defined(REF_MULTI)
+    PANNS::Searching engine;
+    engine.load_data_load(const_cast<char *>(arg_s("data")));
+    engine.load_queries_load(const_cast<char *>(arg_s("queries")));
+    engine.load_common_nsg_graph(const_cast<char *>(arg_s("nsg")));
+    unsigned nq = arg_u("nq", "0");
+    if (nq == 0 || nq > engine.num_queries_) nq = engine.num_queries_;
+    {
+        // Thread split of app/PSS_v5_multi_queries_LG.cpp:89-99 (inner = 8 when
+        // T > 8), or the given inner= (1 = one thread per query).
+        const unsigned inner = arg_u("inner", T > 8 ? "8" : std::to_string(T).c_str());
+        const int outer = std::max(1, T / (int) inner);
+        omp_set_max_active_levels(2);
+        engine.num_threads_inner_ = (int) inner;
+        const unsigned L_local = arg_u("L_local", std::to_string(L).c_str());
+        const unsigned X = arg_u("X", "1");
+        std::vector<std::vector<unsigned>> set_K_list(nq, std::vector<unsigned>(K));
+        std::vector<unsigned> init_ids(L);
+        std::vector<unsigned> local_queues_starts(inner);
+        for (unsigned q_i = 0; q_i < inner; ++q_i) local_queues_starts[q_i] = q_i * L_local;
+        double best = 1e300;
+        unsigned long long n_dist = 0;
+        for (unsigned rep = 0; rep < reps; ++rep) {
+            uint64_t cnt = 0;
+            auto s = std::chrono::high_resolution_clock::now();
+            engine.prepare_init_ids(init_ids, L);
+#pragma omp parallel for num_threads(outer) reduction(+ : cnt)
+            for (unsigned q_i = 0; q_i < nq; ++q_i) {
+                engine.para_search_PSS_v5_multi_queries_LG(q_i, K, L, init_ids, set_K_list[q_i], L_local,
+                                                            local_queues_starts, X, cnt);
+            }
+            auto e = std::chrono::high_resolution_clock::now();
+            double secs = std::chrono::duration<double>(e - s).count();
+            g_rep_times.push_back(secs);
+            if (secs < best) best = secs;
+            n_dist = cnt;
+        }
+        write_ids(arg_s("out"), set_K_list);
+        report(best, n_dist, nq, set_K_list, L, outer * (int) inner);
+        return 0;
+    }
+#elif defined(REF_PSS) || defined(REF_PSS_LG) || defined(REF_TOPM)
     PANNS::Searching engine;
     engine.load_data_load(const_cast<char *>(arg_s("data")));
     engine.load_queries_load(const_cast<char *>(arg_s("queries")));

@@ -132,3 +132,23 @@ def test_pss_workers_against_reference(T, X):
     print(f"T={T} X={X}: recall ours {r_ours:.4f} ref {r_ref:.4f}, mean id overlap {overlap:.4f}")
     assert r_ours >= r_ref - 0.005
     assert overlap > 0.95
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(O.REF_DIR, "ref_multi")),
+                    reason="reference inter-query binary not built here")
+@pytest.mark.parametrize("T", [1, 4])
+def test_reference_inter_query_mode_reproduces_fixtures(T, golden_manifest):
+    """The reference's inter-query PSS_v5 (multi_queries_LG, one thread per
+    query, T queries at a time) returns the LG engine's single-thread ids and
+    distance counts: the CPU baseline runs the same search."""
+    d = os.path.join(GOLDEN, "mix3k_d96")
+    files = dict(data=os.path.join(d, "base.fvecs"), queries=os.path.join(d, "query.fvecs"),
+                 nsg=os.path.join(d, "graph.nsg"))
+    for form in ("lg_t1_L100", "lg_t1_L250"):
+        spec = golden_manifest["mix3k_d96"]["forms"][form]
+        a = spec["args"]
+        with tempfile.TemporaryDirectory() as tmp:
+            ids, st = O.run_ref("ref_multi", os.path.join(tmp, "o.ids"), **files, K=a["K"], L=a["L"], T=T,
+                                X=a["X"], inner=1)
+        assert np.array_equal(ids, golden_ids("mix3k_d96", form, a["K"])), form
+        assert st["n_dist"] == spec["n_dist"], form
