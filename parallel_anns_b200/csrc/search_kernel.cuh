@@ -56,7 +56,15 @@ constexpr uint32_t kIdMask = 0x7fffffffu;
 constexpr uint32_t kFull = 0xffffffffu;
 constexpr int kHeadWords = 32;   // degree + 31 neighbours
 constexpr int kHeadNbrs = kHeadWords - 1;
-constexpr int kBuf = 256;        // fresh-candidate buffer per warp
+#ifndef PANNS_KBUF
+#define PANNS_KBUF 256
+#endif
+#ifndef PANNS_SEARCH_MIN_BLOCKS
+#define PANNS_SEARCH_MIN_BLOCKS 6
+#endif
+constexpr int kBuf = PANNS_KBUF;  // fresh-candidate buffer per warp
+// warp_sort pads a chunk to the next power of two >= its size inside the buffer.
+static_assert(kBuf >= 64 && (kBuf & (kBuf - 1)) == 0, "kBuf must be a power of two >= 64");
 constexpr int kCandGroup = 8;    // candidates whose head rows are staged at once
 constexpr int kGroupChunks = (kCandGroup * kHeadNbrs + 31) / 32;
 constexpr int kMaxM = 64;
@@ -825,7 +833,7 @@ __device__ void search_one(const SearchArgs &a, const WarpMem &m, uint32_t q, ui
 }
 
 template <int KIND, int ORDER, int CL, int STORE>
-__global__ void __launch_bounds__(128, 6) search_kernel(SearchArgs a) {
+__global__ void __launch_bounds__(128, PANNS_SEARCH_MIN_BLOCKS) search_kernel(SearchArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
     const int lane = threadIdx.x & 31;
     const int wid = threadIdx.x >> 5;

@@ -83,11 +83,12 @@ def load(build_if_missing: bool = True):
     global _lib
     if _lib is not None:
         return _lib
-    if build_if_missing:
+    path = os.environ.get("PANNS_B200_LIB") or _build.SO  # another build of the same library
+    if build_if_missing and path == _build.SO:
         _build.build()
-    if not os.path.exists(_build.SO):
-        raise PannsError(-4, f"native library not built: {_build.SO}")
-    L = ctypes.CDLL(_build.SO)
+    if not os.path.exists(path):
+        raise PannsError(-4, f"native library not built: {path}")
+    L = ctypes.CDLL(path)
     P = ctypes.c_void_p
     u32 = ctypes.c_uint32
     i32 = ctypes.c_int
