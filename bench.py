@@ -229,12 +229,12 @@ def bench_ours(args):
     choices = None
     if fixed:
         c = {"storage": args.storage or 0, "M": args.M, "L": args.L, "warps_per_block": args.wpb,
-             "learned": None, "blocks_per_sm": 0}
+             "learned": None, "blocks_per_sm": 0, "warps_per_query": 1}
         choices = {"plain": dict(c, storage=0), "head": c, "tables": []}
     elif rank == 0:
         t0 = time.time()
         plain = AT.tune(handles[N.STORE_FP32], tune_q, tune_gt, K=K, target=RECALL_TARGET,
-                        storages=(N.STORE_FP32,), Ms=Ms, wpbs=(2, 4))
+                        storages=(N.STORE_FP32,), Ms=Ms, wpbs=(2, 4), wpqs=(1, 2, 4))
         cands = [plain]
         for store in stores:
             if store == N.STORE_FP32 and model is None:
@@ -291,8 +291,9 @@ def bench_ours(args):
         learned_info = {"options": head.learned, "fallback_rate": round(float(fb.mean()), 4),
                         "mean_L": round(float(Lq.mean()), 1), "R": model.R,
                         "training_queries": 200_000}
-    if (plain.storage, plain.L, plain.M, plain.learned, plain.warps_per_block) == (
-            head.storage, head.L, head.M, head.learned, head.warps_per_block):
+    if (plain.storage, plain.L, plain.M, plain.learned, plain.warps_per_block, plain.warps_per_query,
+            plain.blocks_per_sm) == (head.storage, head.L, head.M, head.learned, head.warps_per_block,
+                                     head.warps_per_query, head.blocks_per_sm):
         p_ms, p_ids, p_tot = kernel_ms, last_ids, tot
     else:
         p_ms, p_tot, p_ids = timed(plain)
@@ -321,24 +322,35 @@ def bench_ours(args):
     # Batch sizes 1, 64 and 1000 through the asynchronous device-pointer entry
     # point with the CUDA-graph-captured launch, batches back to back on one
     # stream (device time from the first launch to the last result).
+    # Per batch size the warps per query is tuned too (1, 2, 4; several warps
+    # only for the plain FP32 search), at the head's L and M.
     batching = {}
     qd = torch.from_numpy(qs).cuda()
     stream = torch.cuda.Stream()
     for B, nb in ((1, 300), (64, 60), (1000, 10)):
         outb = torch.empty((B, K), dtype=torch.int32, device="cuda")
-        kwb = dict(kw, flags=kw["flags"] | N.FLAG_CUDA_GRAPH)
-        for i in range(3):
-            ixh.search_device(qd[i * B:(i + 1) * B], outb, K=K, stream=stream, **kwb)
-        stream.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for i in range(nb):
-            s0 = (i * B) % (nq - B + 1)
-            ixh.search_device(qd[s0:s0 + B], outb, K=K, stream=stream, **kwb)
-        e1.record(stream)
-        stream.synchronize()
-        ms = e0.elapsed_time(e1)
-        batching[str(B)] = {"qps": round(nb * B / (ms / 1e3), 1), "ms_per_batch": round(ms / nb, 4)}
+        best_b = None
+        wpq_options = [1]
+        if head.storage == N.STORE_FP32 and head.learned is None:
+            wpq_options += [2, 4]
+        for wq in wpq_options:
+            kwb = dict(kw, flags=kw["flags"] | N.FLAG_CUDA_GRAPH, warps_per_query=wq)
+            for i in range(3):
+                ixh.search_device(qd[i * B:(i + 1) * B], outb, K=K, stream=stream, **kwb)
+            stream.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for i in range(nb):
+                s0 = (i * B) % (nq - B + 1)
+                ixh.search_device(qd[s0:s0 + B], outb, K=K, stream=stream, **kwb)
+            e1.record(stream)
+            stream.synchronize()
+            ms = e0.elapsed_time(e1)
+            r_ = {"qps": round(nb * B / (ms / 1e3), 1), "ms_per_batch": round(ms / nb, 4), "warps_per_query": wq}
+            if best_b is None or r_["qps"] > best_b["qps"]:
+                best_b = dict(r_, tried={})
+            best_b["tried"][str(wq)] = r_["qps"]
+        batching[str(B)] = best_b
     batching[str(nq)] = {"qps": round(nq * args.steps / (kernel_ms / 1e3), 1),
                          "ms_per_batch": round(kernel_ms / args.steps, 4)}
 
@@ -393,7 +405,8 @@ def bench_ours(args):
             "config": {"workload": "batched search, 1M x 96d mixture64 (sigma 0.3, unit norm), "
                                    "NSG-style graph R=50, 10k queries per GPU, K=100",
                        "n": args.n, "d": d, "queries_per_gpu": nq, "K": K, "L": L, "M": M,
-                       "warps_per_block": head.warps_per_block,
+                       "warps_per_block": head.warps_per_block, "warps_per_query": head.warps_per_query,
+                       "blocks_per_sm": head.blocks_per_sm,
                        "storage": names[store], "accumulate": "f32",
                        "rerank": "exact f32 of the final L" if store != N.STORE_FP32 else None,
                        "learned": learned_info,
@@ -417,6 +430,7 @@ def bench_ours(args):
             "gpu_launches": steps,
             "plain_fp32": {"value": round(nq * world * steps / (p_ms_max / 1e3), 1), "unit": UNIT,
                            "L": plain.L, "M": plain.M, "warps_per_block": plain.warps_per_block,
+                           "warps_per_query": plain.warps_per_query,
                            "recall100": round(p_rec, 5), "ms_per_step": round(p_ms_max / steps, 4),
                            "roofline_frac": round(p_alg / (p_ms / steps / 1e3) / 1e9 / peak, 4)},
             "batching": batching,

@@ -86,6 +86,10 @@ typedef struct {
                                 call, PSS.cpp:1218). */
     uint32_t blocks_per_sm;  /* resident blocks per SM (0 = as many as fit); fewer leave more of
                                 the SM's L1 / shared array to L1, which caches gathered rows */
+    uint32_t warps_per_query; /* 0 or 1: one warp per query (warps_per_block queries per block);
+                                 2 or 4: that many warps share each query's steps (one query per
+                                 block; NSG_SEQ, TOP_M, PSS_V5 at T = 1, FP32 storage), for small
+                                 batches; same ids and counts */
 } panns_search_params;
 
 /* Enqueue the launch (per-call memsets, query layout and the search kernel)

@@ -6,9 +6,10 @@ learned model is given, whether and how to use it, by measuring.
 
 Procedure, per candidate (storage, M, learned option): the smallest L of a
 grid whose recall on the tuning queries meets the target (binary search; the
-recall of a search grows with L), then the warps per block and resident
-blocks per SM (which sets how much of each SM's L1 / shared array is left to
-L1) that run it fastest; the fastest candidate wins. Times are the search kernel's CUDA-event
+recall of a search grows with L), then the block shape that runs it fastest:
+warps per block and resident blocks per SM (which sets how much of each SM's
+L1 / shared array is left to L1) with one warp per query, or 2 / 4 warps per
+query (one query per block, for small batches); the fastest candidate wins. Times are the search kernel's CUDA-event
 time, best of ``reps``. Evaluate the result on other queries than the tuning
 ones. Choices are cached per shape in a JSON file when ``cache`` is given.
 """
@@ -33,6 +34,7 @@ class Choice:
     warps_per_block: int
     learned: dict | None = None      # options of learned.attach, or None for the plain search
     blocks_per_sm: int = 0           # resident blocks per SM (0 = as many as fit)
+    warps_per_query: int = 1         # 1: one warp per query; 2 / 4: one query per block of that many warps
     recall: float = 0.0
     kernel_ms: float = 0.0
     qps: float = 0.0
@@ -42,7 +44,7 @@ class Choice:
         from . import native as _N
         return dict(L=self.L, M=self.M, mode=_N.MODE_NSG_SEQ if self.M == 1 else _N.MODE_TOP_M,
                     storage=self.storage, warps_per_block=self.warps_per_block,
-                    blocks_per_sm=self.blocks_per_sm,
+                    blocks_per_sm=self.blocks_per_sm, warps_per_query=self.warps_per_query,
                     flags=_N.FLAG_LEARNED if self.learned is not None else 0)
 
 
@@ -55,14 +57,14 @@ def _time(index, queries, K, kw, reps):
 
 
 def tune(index, queries, gt, *, K=100, target=0.95, storages=(N.STORE_FP32,), Ms=(1, 2, 4, 8, 16),
-         wpbs=(2, 4), bpss=(0, 5, 4), learned_model=None, learned_opts=(), include_plain=True,
+         wpbs=(2, 4), bpss=(0, 5, 4), wpqs=(1,), learned_model=None, learned_opts=(), include_plain=True,
          L_grid=L_GRID, reps=2, cache=None, log=None) -> Choice:
     from . import learned as LE
     from .searching import recall
     key = None
     if cache:
         key = json.dumps({"n": index.n, "d": index.d, "nq": int(queries.shape[0]), "K": K, "target": target,
-                          "storages": list(storages), "Ms": list(Ms), "wpbs": list(wpbs), "bpss": list(bpss),
+                          "storages": list(storages), "Ms": list(Ms), "wpbs": list(wpbs), "bpss": list(bpss), "wpqs": list(wpqs),
                           "learned": [dict(o) for o in learned_opts] if learned_model is not None else [],
                           "plain": include_plain, "grid": list(L_grid)}, sort_keys=True)
         if os.path.exists(cache):
@@ -100,17 +102,19 @@ def tune(index, queries, gt, *, K=100, target=0.95, storages=(N.STORE_FP32,), Ms
                     else:
                         lo = mid + 1
                 L = L_grid[lo]
-                for w in wpbs:
-                    for bps in bpss:
-                        # blocks_per_sm counts blocks of w warps: keep the warps per SM comparable
-                        b = bps * 4 // w if bps else 0
-                        kw2 = dict(kw, warps_per_block=w, blocks_per_sm=b)
-                        _, ms = _time(index, queries, K, dict(kw2, L=L), reps)
-                        row = {"storage": store, "M": M, "learned": opt, "L": L, "warps_per_block": w,
-                               "blocks_per_sm": b, "recall": rec(L), "kernel_ms": ms}
-                        table.append(row)
-                        if best is None or ms < best.kernel_ms:
-                            best = Choice(store, M, L, w, opt, b, rec(L), ms, queries.shape[0] / (ms / 1e3))
+                shapes = [(w, bps, 1) for w in wpbs for bps in bpss]
+                if store == N.STORE_FP32 and opt is None:  # several warps per query: FP32, plain only
+                    shapes += [(wq, 0, wq) for wq in wpqs if wq > 1]
+                for w, bps, wq in shapes:
+                    # blocks_per_sm counts blocks of w warps: keep the warps per SM comparable
+                    b = bps * 4 // w if bps else 0
+                    kw2 = dict(kw, warps_per_block=w, blocks_per_sm=b, warps_per_query=wq)
+                    _, ms = _time(index, queries, K, dict(kw2, L=L), reps)
+                    row = {"storage": store, "M": M, "learned": opt, "L": L, "warps_per_block": w,
+                           "blocks_per_sm": b, "warps_per_query": wq, "recall": rec(L), "kernel_ms": ms}
+                    table.append(row)
+                    if best is None or ms < best.kernel_ms:
+                        best = Choice(store, M, L, w, opt, b, wq, rec(L), ms, queries.shape[0] / (ms / 1e3))
                 if log:
                     log(f"autotune storage={store} M={M} learned={opt}: L={L} recall={rec(L):.4f} "
                         f"ms={min(r['kernel_ms'] for r in table if r.get('L') == L and r['M'] == M and r['storage'] == store and r['learned'] == opt):.3f}")

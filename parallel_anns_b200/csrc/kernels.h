@@ -27,6 +27,9 @@ inline const void *search_kernel_ptr(uint32_t kind, uint32_t order, int CL, uint
     if (store == 2) return search_kernel_ptr_fp8(kind, order, CL);
     return kind == 0 ? search_kernel_ptr_fp32_ip(kind, order, CL) : search_kernel_ptr_fp32_l2(kind, order, CL);
 }
+// search_block_kernel<KIND, CL, W> (block_kernel.cuh), W warps per query;
+// nullptr if not built (W other than 2 and 4).
+const void *search_block_kernel_ptr(uint32_t kind, int CL, uint32_t W);
 // pss_kernel<KIND, CL> (pss_kernel.cuh); nullptr if not built.
 const void *pss_kernel_ptr(uint32_t kind, int CL);
 

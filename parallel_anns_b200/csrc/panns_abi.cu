@@ -17,6 +17,7 @@
 #include "../../include/panns_learned.h"
 #include "learned.h"
 #include "search_kernel.cuh"
+#include "block_kernel.cuh"
 #include "gt_kernel.cuh"
 #include "pss_kernel.cuh"
 #include "kernels.h"
@@ -166,7 +167,7 @@ struct panns_index {
     std::vector<uint32_t> perm, inv;  // device id -> original id, and back
     DevBuf<uint32_t> orig;
     // graph
-    uint32_t width = 0, entry = 0, gn = 0;
+    uint32_t width = 0, entry = 0, gn = 0, max_deg = 0;
     std::vector<uint64_t> off;
     std::vector<uint32_t> nbrs;
     DevBuf<uint32_t> head, ovf;
@@ -366,6 +367,8 @@ int panns_set_graph(panns_index *h, uint32_t width, uint32_t entry, const uint64
                                           " >= N");
     h->off.assign(offsets, offsets + n + 1);
     h->nbrs.assign(nbrs, nbrs + E);
+    h->max_deg = 0;
+    for (uint32_t v = 0; v < n; ++v) h->max_deg = std::max<uint32_t>(h->max_deg, (uint32_t) (offsets[v + 1] - offsets[v]));
     h->width = width;
     h->entry = entry;
     h->gn = n;
@@ -641,6 +644,17 @@ int check_params(panns_index *h, const panns_search_params *p) {
     if (p->L_query && p->mode == PANNS_MODE_PSS_V5 && p->T > 1)
         return fail(PANNS_EINVAL, "search: L_query is not supported by PSS_V5 with T > 1");
     if (p->storage > PANNS_STORE_FP8) return fail(PANNS_EINVAL, "search: unknown storage");
+    if (p->warps_per_query > 1) {
+        if (p->warps_per_query != 2 && p->warps_per_query != 4)
+            return fail(PANNS_EINVAL, "search: warps_per_query must be 0, 1, 2 or 4");
+        const bool ok = p->mode == PANNS_MODE_NSG_SEQ || p->mode == PANNS_MODE_TOP_M ||
+                        (p->mode == PANNS_MODE_PSS_V5 && p->T == 1);
+        if (!ok || p->storage != PANNS_STORE_FP32 || (p->flags & PANNS_FLAG_LEARNED))
+            return fail(PANNS_EINVAL, "search: warps_per_query > 1 is for NSG_SEQ, TOP_M and PSS_V5 at T = 1 "
+                                      "with float32 storage, without PANNS_FLAG_LEARNED");
+        if (h->max_deg > (uint32_t) kBuf)
+            return fail(PANNS_EINVAL, "search: warps_per_query > 1 needs a graph degree <= " + std::to_string(kBuf));
+    }
     if (p->storage != PANNS_STORE_FP32) {
         if (p->storage != h->storage)
             return fail(PANNS_EINVAL, "search: that reduced copy was not built (panns_set_base storage)");
@@ -757,7 +771,9 @@ static int launch_search(panns_index *h, const panns_search_params *p, float *d_
     const uint32_t order = p->mode == PANNS_MODE_EFANNA ? ORDER_EFANNA : ORDER_PANNS;
     const uint32_t kind = p->distance == PANNS_DIST_L2 ? KIND_L2 : KIND_IP;
     const bool pss = p->mode == PANNS_MODE_PSS_V5 && p->T > 1;
-    const void *kern = pss ? pss_kernel_ptr(kind, CL) : search_kernel_ptr(kind, order, CL, p->storage);
+    const uint32_t wpq = p->warps_per_query > 1 ? p->warps_per_query : 1u;
+    const void *kern = wpq > 1 ? search_block_kernel_ptr(kind, CL, wpq)
+                               : pss ? pss_kernel_ptr(kind, CL) : search_kernel_ptr(kind, order, CL, p->storage);
     if (!kern) return fail(PANNS_EINVAL, "search: unsupported dimension");
     const uint32_t M = p->mode == PANNS_MODE_TOP_M ? p->M : 1u;
     uint32_t qcap = ((p->L + 31) / 32) * 32;
@@ -767,14 +783,17 @@ static int launch_search(panns_index *h, const panns_search_params *p, float *d_
     }
     const uint32_t L_local = p->L_local ? p->L_local : p->L;
     const uint32_t wcap = ((L_local + 31) / 32) * 32;
-    uint32_t wpb = p->warps_per_block ? p->warps_per_block : 4u;
+    // Block shape: wpb queries of one warp each, or one query of wpq warps.
+    uint32_t wpb = wpq > 1 ? wpq : (p->warps_per_block ? p->warps_per_block : 4u);
     size_t per_warp = pss ? pss_smem_bytes(qcap, p->T, wcap) : warp_smem_bytes(qcap);
     if (pss && !p->warps_per_block) {
         while (wpb > 1 && wpb * per_warp > (100u << 10)) --wpb;
     }
     if (per_warp > (227u << 10))
         return fail(PANNS_EINVAL, "search: the queues (L, T x L_local) do not fit in shared memory");
-    const size_t smem = (size_t) wpb * per_warp;
+    const size_t smem = wpq > 1 ? (size_t) block_smem_bytes(qcap, wpq) : (size_t) wpb * per_warp;
+    if (smem > (227u << 10)) return fail(PANNS_EINVAL, "search: the queue does not fit in shared memory");
+    const uint32_t qpb = wpq > 1 ? 1u : wpb;  // queries in flight per block
     {
         cudaFuncAttributes fa;
         CU(cudaFuncGetAttributes(&fa, kern));
@@ -794,16 +813,16 @@ static int launch_search(panns_index *h, const panns_search_params *p, float *d_
     if (per_sm < 1) return fail(PANNS_EINVAL, "search: L too large for shared memory");
     if (p->blocks_per_sm) per_sm = std::min(per_sm, (int) p->blocks_per_sm);
     uint32_t blocks = (uint32_t) per_sm * (uint32_t) h->num_sms;
-    const uint32_t need_blocks = (nq + wpb - 1) / wpb;
+    const uint32_t need_blocks = (nq + qpb - 1) / qpb;
     blocks = std::max(1u, std::min(blocks, need_blocks));
     // Per-slot visited bitsets (bounded to 16 GiB) and dirty-word lists.
     const uint32_t vis_words = (h->n + 31) / 32;
     const uint32_t dirty_cap = 8192;
-    if ((uint64_t) blocks * wpb * vis_words * 4 > (16ull << 30)) {
+    if ((uint64_t) blocks * qpb * vis_words * 4 > (16ull << 30)) {
         const uint32_t max_slots = (uint32_t) ((16ull << 30) / (vis_words * 4ull));
-        blocks = std::max(1u, max_slots / wpb);
+        blocks = std::max(1u, max_slots / qpb);
     }
-    const uint32_t nslots = blocks * wpb;
+    const uint32_t nslots = blocks * qpb;
     if (h->vis_slots < nslots || h->vis_words != vis_words) {
         CU(h->visited.ensure((size_t) nslots * vis_words));
         CU(cudaMemsetAsync(h->visited.p, 0, (size_t) nslots * vis_words * 4, stream));
@@ -867,6 +886,9 @@ static int launch_search(panns_index *h, const panns_search_params *p, float *d_
     a.counter = h->counter.p;
     a.error = h->error.p;
     a.queue_cap = qcap;
+    // Block kernel: candidates per warp and merge round, so that a warp's
+    // fresh neighbours (at most max_deg per candidate) fit its list.
+    a.block_round = std::max(1u, std::min<uint32_t>(kCandGroup, kBuf / std::max(1u, h->max_deg)));
     PssArgs pa;
     memset(&pa, 0, sizeof(pa));
     memcpy(&pa.s, &a, sizeof(a));

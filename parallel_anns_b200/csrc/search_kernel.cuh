@@ -108,6 +108,7 @@ struct SearchArgs {
     uint32_t d;               // dimension
     const uint32_t *Lq;       // per-query queue length (K <= Lq[q] <= L), or null: L for all
     const MlpDev *mlp;        // entry / L-budget network run in the prologue, or null
+    uint32_t block_round;     // search_block_kernel: candidates per warp and merge round
 };
 
 // Bytes of shared memory one warp needs.

@@ -49,7 +49,8 @@ FLAG_LEARNED = 2
 class SearchParams(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint32) for n in
                 ("mode", "distance", "K", "L", "M", "T", "L_local", "X", "warps_per_block", "storage",
-                 "flags")] + [("L_query", ctypes.c_void_p), ("blocks_per_sm", ctypes.c_uint32)]
+                 "flags")] + [("L_query", ctypes.c_void_p), ("blocks_per_sm", ctypes.c_uint32),
+                              ("warps_per_query", ctypes.c_uint32)]
 
 
 class MlpTrainParams(ctypes.Structure):

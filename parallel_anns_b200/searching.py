@@ -115,24 +115,24 @@ class Index:
     @staticmethod
     def params(mode=N.MODE_NSG_SEQ, distance=N.DIST_NORM_IP, K=100, L=100, M=1, T=1,
                L_local=0, X=1, warps_per_block=0, storage=N.STORE_FP32, flags=0,
-               L_query=None, blocks_per_sm=0) -> N.SearchParams:
+               L_query=None, blocks_per_sm=0, warps_per_query=0) -> N.SearchParams:
         """Search parameters. ``L_query``, if given, must be a C-contiguous
         uint32 array kept alive by the caller until the call returns."""
         lq = None if L_query is None else L_query.ctypes.data
         return N.SearchParams(mode, distance, K, L, M, T, L_local, X, warps_per_block, storage, flags, lq,
-                              blocks_per_sm)
+                              blocks_per_sm, warps_per_query)
 
     def search(self, queries: np.ndarray | None = None, *, K=100, L=100, mode=N.MODE_NSG_SEQ,
                distance=N.DIST_NORM_IP, M=1, T=1, L_local=0, X=1, init_ids=None,
                q_begin=0, nq=None, warps_per_block=0, storage=N.STORE_FP32, flags=0, L_query=None,
-               blocks_per_sm=0):
+               blocks_per_sm=0, warps_per_query=0):
         """Search a batch. With ``queries`` None the loaded queries
         [q_begin, q_begin + nq) are used. ``L_query``: optional per-query
         queue lengths (K <= L_query[i] <= L). Returns (ids [nq x K], stats dict)."""
         if L_query is not None:
             L_query = np.ascontiguousarray(L_query, dtype=np.uint32)
         p = self.params(mode, distance, K, L, M, T, L_local, X, warps_per_block, storage, flags, L_query,
-                        blocks_per_sm)
+                        blocks_per_sm, warps_per_query)
         st = N.Stats()
         ii = None
         if init_ids is not None:
@@ -154,7 +154,7 @@ class Index:
     def search_device(self, queries, out, *, K=100, L=100, mode=N.MODE_NSG_SEQ,
                       distance=N.DIST_NORM_IP, M=1, T=1, L_local=0, X=1, init_ids=None,
                       warps_per_block=0, storage=N.STORE_FP32, flags=0, L_query=None, stream=None,
-                      blocks_per_sm=0):
+                      blocks_per_sm=0, warps_per_query=0):
         """Asynchronous search of device queries (a torch float32 CUDA tensor,
         nq x d) into ``out`` (a torch int32/uint32 CUDA tensor, nq x K, original
         ids), enqueued on ``stream`` (a torch.cuda.Stream; None = the handle's
@@ -162,7 +162,7 @@ class Index:
         if L_query is not None:
             L_query = np.ascontiguousarray(L_query, dtype=np.uint32)
         p = self.params(mode, distance, K, L, M, T, L_local, X, warps_per_block, storage, flags, L_query,
-                        blocks_per_sm)
+                        blocks_per_sm, warps_per_query)
         ii = None if init_ids is None else np.ascontiguousarray(init_ids, dtype=np.uint32)
         s = None if stream is None else ctypes.c_void_p(stream.cuda_stream)
         N.check(self._lib.panns_search_device(self._h, ctypes.byref(p), ctypes.c_void_p(queries.data_ptr()),

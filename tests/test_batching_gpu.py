@@ -12,6 +12,12 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.fixture(scope="module")
+def N_lib():
+    from parallel_anns_b200 import native as N
+    return N
+
+
+@pytest.fixture(scope="module")
 def setup():
     from parallel_anns_b200 import datasets as ds
     from parallel_anns_b200 import native as N
@@ -121,3 +127,59 @@ def test_autotuner_meets_target_on_tuning_queries(setup):
     rows = [r for r in c.table if r.get("L")]
     assert all(r["recall"] >= 0.97 for r in rows)
     assert c.kernel_ms == min(r["kernel_ms"] for r in rows)
+
+
+@pytest.mark.parametrize("wpq", [2, 4])
+@pytest.mark.parametrize("mode,M,L,dist", [(0, 1, 100, 0), (1, 4, 200, 0), (1, 8, 300, 1), (1, 64, 160, 0),
+                                          (2, 1, 257, 1)])
+def test_several_warps_per_query_equal_one(setup, wpq, mode, M, L, dist):
+    """warps_per_query 2 / 4 return the one-warp kernel's ids and counts (and the oracle's)."""
+    ix, N, base, q, g = setup
+    K = min(100, L)
+    ref, st = ix.search(K=K, L=L, mode=mode, M=M, distance=dist)
+    got, st2 = ix.search(K=K, L=L, mode=mode, M=M, distance=dist, warps_per_query=wpq)
+    assert np.array_equal(got, ref)
+    assert st2["n_dist"] == st["n_dist"] and st2["n_iter"] == st["n_iter"]
+    assert st2["n_edges"] == st["n_edges"] and st2["n_expand"] == st["n_expand"]
+    if mode == 1 and M == 8:
+        G = O.Graph.from_nsg(g)
+        oref, nd = O.search_top_m(base, G, q[:40], K, L, M, kind=O.DIST_L2)
+        assert np.array_equal(got[:40], oref)
+
+
+def test_several_warps_per_query_small_batches_and_per_query_L(setup):
+    import torch
+    ix, N, base, q, g = setup
+    Lq = np.random.default_rng(3).choice([64, 100, 200], size=q.shape[0]).astype(np.uint32)
+    ref, _ = ix.search(K=50, L=200, mode=1, M=8, L_query=Lq)
+    got, _ = ix.search(K=50, L=200, mode=1, M=8, L_query=Lq, warps_per_query=4)
+    assert np.array_equal(got, ref)
+    qd = torch.from_numpy(q[:5]).cuda()
+    out = torch.full((5, 50), -1, dtype=torch.int32, device="cuda")
+    for i in range(5):
+        ix.search_device(qd[i:i + 1], out[i:i + 1], K=50, L=200, mode=1, M=8, warps_per_query=4,
+                         flags=N.FLAG_CUDA_GRAPH)
+    torch.cuda.synchronize()
+    ref5, _ = ix.search(q[:5], K=50, L=200, mode=1, M=8)
+    assert np.array_equal(out.cpu().numpy().view(np.uint32), ref5)
+    with pytest.raises(N.PannsError):
+        ix.search(K=50, L=200, warps_per_query=3)
+    with pytest.raises(N.PannsError):
+        ix.search(K=50, L=200, mode=N.MODE_EFANNA, warps_per_query=2)
+
+
+@pytest.mark.parametrize("d", [8, 24, 128, 256])
+def test_several_warps_per_query_dimensions(N_lib, d):
+    from parallel_anns_b200 import datasets as ds
+    from parallel_anns_b200.searching import Index
+    base = ds.gaussian_mixture(3000, d, seed=d, means_seed=d)
+    q = ds.gaussian_mixture(64, d, seed=d + 1, means_seed=d)
+    g = ds.build_nsg_graph(base, R=32, knn_k=40, device="cpu")
+    with Index(0) as ix:
+        ix.set_base(base)
+        ix.set_graph(g)
+        ix.set_queries(q)
+        for dist in (0, 1):
+            ref, st = ix.search(K=50, L=120, mode=1, M=4, distance=dist)
+            got, st2 = ix.search(K=50, L=120, mode=1, M=4, distance=dist, warps_per_query=2)
+            assert np.array_equal(got, ref) and st["n_dist"] == st2["n_dist"]
