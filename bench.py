@@ -329,7 +329,7 @@ def bench_ours(args):
     stream = torch.cuda.Stream()
     for B, nb in ((1, 300), (64, 60), (1000, 10)):
         outb = torch.empty((B, K), dtype=torch.int32, device="cuda")
-        best_b = None
+        best_b, tried = None, {}
         wpq_options = [1]
         if head.storage == N.STORE_FP32 and head.learned is None:
             wpq_options += [2, 4]
@@ -347,10 +347,10 @@ def bench_ours(args):
             stream.synchronize()
             ms = e0.elapsed_time(e1)
             r_ = {"qps": round(nb * B / (ms / 1e3), 1), "ms_per_batch": round(ms / nb, 4), "warps_per_query": wq}
+            tried[str(wq)] = r_["qps"]
             if best_b is None or r_["qps"] > best_b["qps"]:
-                best_b = dict(r_, tried={})
-            best_b["tried"][str(wq)] = r_["qps"]
-        batching[str(B)] = best_b
+                best_b = r_
+        batching[str(B)] = dict(best_b, qps_by_warps_per_query=tried)
     batching[str(nq)] = {"qps": round(nq * args.steps / (kernel_ms / 1e3), 1),
                          "ms_per_batch": round(kernel_ms / args.steps, 4)}
 

@@ -156,7 +156,7 @@ __device__ void block_search_one(const SearchArgs &a, uint32_t q, uint8_t *smem,
     // Distances, filter against the queue's L-th (bound), keys, sort; leaves
     // the warp's survivor count in ctl[BC_SEG + w].
     auto finish_list = [&](uint32_t nb, bool filter) {
-        D.distances(a, bi, bd, nb, lane);
+        distances_wide<KIND, CL>(a, D.qv, bi, bd, nb, lane);
         if (lane == 0 && nb) atomicAdd(&ctl[BC_DIST], nb);
         const uint32_t sz = ctl[BC_SZ];
         const bool any_bound = filter && sz >= L;
@@ -286,8 +286,12 @@ __device__ void block_search_one(const SearchArgs &a, uint32_t q, uint8_t *smem,
             if (lane == 0 && gc) atomicAdd(&ctl[BC_EDGES], gc + degsum);
             const bool any_long = __any_sync(kFull, deg > (uint32_t) kHeadNbrs);
             __syncwarp();
-            for (uint32_t f0 = 0; f0 < total; f0 += 32) {
-                const uint32_t f = f0 + lane;
+            // Head-row neighbours: every visited test-and-set of the round is
+            // issued before any result is used (total <= kCandGroup * 31).
+            uint32_t ids[kGroupChunks], olds[kGroupChunks];
+#pragma unroll
+            for (int ch = 0; ch < kGroupChunks; ++ch) {
+                const uint32_t f = ch * 32 + lane;
                 uint32_t id = 0;
                 bool valid = f < total;
                 if (valid) {
@@ -299,9 +303,16 @@ __device__ void block_search_one(const SearchArgs &a, uint32_t q, uint8_t *smem,
                         valid = false;
                     }
                 }
-                const uint32_t old = visit_issue(vis, id, valid);
-                const bool fresh = valid && !(old & (1u << (id & 31)));
-                note_dirty_block(valid && old == 0, id >> 5);
+                ids[ch] = valid ? id : kFull;
+                olds[ch] = visit_issue(vis, id, valid);
+            }
+#pragma unroll
+            for (int ch = 0; ch < kGroupChunks; ++ch) {
+                if (ch * 32 >= (int) total) break;
+                const uint32_t id = ids[ch];
+                const bool valid = id != kFull;
+                const bool fresh = valid && !(olds[ch] & (1u << (id & 31)));
+                note_dirty_block(valid && olds[ch] == 0, id >> 5);
                 const uint32_t bm = __ballot_sync(kFull, fresh);
                 if (fresh) bi[nb + __popc(bm & lanemask_lt())] = id;
                 nb += __popc(bm);

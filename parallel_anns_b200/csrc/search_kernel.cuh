@@ -452,6 +452,41 @@ struct Dist<KIND, CL, STORE_FP32> {
     }
 };
 
+// Four vertices per 8-lane group (16 per warp pass), all rows loaded before
+// any is used: the same per-vertex arithmetic as group_distance2, with twice
+// the loads in flight, for kernels with registers to spare.
+template <int KIND, int CL>
+__device__ __forceinline__ void distances_wide(const SearchArgs &a, const float4 (&qv)[CL], const uint32_t *ids,
+                                               float *out, uint32_t nb, int lane) {
+    const int g = lane >> 3, c = lane & 7;
+    for (uint32_t b0 = 0; b0 < nb; b0 += 16) {
+        uint32_t v[4];
+        bool act[4];
+        float4 x[4][CL];
+        float nrm[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const uint32_t b = b0 + 4 * u + g;
+            act[u] = b < nb;
+            v[u] = act[u] ? ids[b] & kIdMask : 0u;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const float4 *r = a.vec + (size_t) v[u] * (CL * 8) + c;
+#pragma unroll
+            for (int i = 0; i < CL; ++i) x[u][i] = act[u] ? __ldg(r + 8 * i) : make_float4(0.f, 0.f, 0.f, 0.f);
+            nrm[u] = (KIND == KIND_IP && act[u]) ? __ldg(a.norms + v[u]) : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            float s = lane_sum8(chain<KIND, CL>(x[u], qv), lane);
+            if (KIND == KIND_IP) s = __fmaf_rn(-2.0f, s, nrm[u]);
+            if (c == 0 && act[u]) out[b0 + 4 * u + g] = s;
+        }
+    }
+    __syncwarp();
+}
+
 // Position of natural element e in a chain-major padded row (inverse of the
 // layout's chain_term_element).
 static __device__ __forceinline__ int chain_major_pos(int d, int e) {
