@@ -776,11 +776,7 @@ static int launch_search(panns_index *h, const panns_search_params *p, float *d_
                                : pss ? pss_kernel_ptr(kind, CL) : search_kernel_ptr(kind, order, CL, p->storage);
     if (!kern) return fail(PANNS_EINVAL, "search: unsupported dimension");
     const uint32_t M = p->mode == PANNS_MODE_TOP_M ? p->M : 1u;
-    uint32_t qcap = ((p->L + 31) / 32) * 32;
-    if (p->storage != PANNS_STORE_FP32) {  // the re-rank sorts the queue in place
-        qcap = 32;
-        while (qcap < p->L) qcap <<= 1;
-    }
+    const uint32_t qcap = ((p->L + 31) / 32) * 32;
     const uint32_t L_local = p->L_local ? p->L_local : p->L;
     const uint32_t wcap = ((L_local + 31) / 32) * 32;
     // Block shape: wpb queries of one warp each, or one query of wpq warps.

@@ -59,6 +59,9 @@ constexpr int kHeadNbrs = kHeadWords - 1;
 #ifndef PANNS_KBUF
 #define PANNS_KBUF 256
 #endif
+#ifndef PANNS_WIDE_DIST
+#define PANNS_WIDE_DIST 0  // 1: 16 rows in flight per warp pass in the one-warp kernel too
+#endif
 #ifndef PANNS_SEARCH_MIN_BLOCKS
 #define PANNS_SEARCH_MIN_BLOCKS 6
 #endif
@@ -100,8 +103,7 @@ struct SearchArgs {
     uint32_t dirty_cap;
     uint32_t *counter;        // work-stealing query counter
     uint32_t *error;          // ERR_* bits
-    uint32_t queue_cap;       // shared-memory queue entries per warp (>= L; a power of
-                              // two >= L when a reduced copy is searched)
+    uint32_t queue_cap;       // shared-memory queue entries per warp (>= L, a multiple of 32)
     const void *vec_lo;       // reduced rows, natural element order: n x dpad (BF16 or FP8)
     const float *norms_lo;    // ||v||^2 of the dequantised rows
     const float *scales;      // FP8: per-dimension scale (dpad)
@@ -621,13 +623,60 @@ static __device__ void rank_sort(float *qd, uint32_t *qi, uint32_t sz, const uin
     }
 }
 
+// Order the sz entries (qd, qi) by (distance, original id) and write the
+// original ids of the first K to out. The entries are cut into runs whose
+// sizes are the binary digits of sz (largest first); each run is sorted in
+// place by rank_sort (a power of two, so it needs no padding) and an entry's
+// output position is its index in its run plus, for every other run, the
+// number of that run's entries that precede it. The queue therefore needs no
+// room beyond sz.
+static __device__ void rerank_output(float *qd, uint32_t *qi, uint32_t sz, uint32_t K, const uint32_t *orig,
+                                     uint32_t *out, int lane) {
+    for (uint32_t start = 0, b = 32; b-- > 0;) {
+        const uint32_t n = 1u << b;
+        if (!(sz & n)) continue;
+        rank_sort(qd + start, qi + start, n, orig, lane);
+        start += n;
+    }
+    __syncwarp();
+    for (uint32_t i = lane; i < sz; i += 32) {
+        const float d = qd[i];
+        const uint32_t key = __ldg(orig + (qi[i] & kIdMask));
+        uint32_t rank = 0;
+        for (uint32_t start = 0, b = 32; b-- > 0;) {
+            const uint32_t n = 1u << b;
+            if (!(sz & n)) continue;
+            if (i >= start && i < start + n) {
+                rank += i - start;
+            } else {
+                uint32_t lo = 0, hi = n;
+                while (lo < hi) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    const float md = qd[start + mid];
+                    const bool before = md < d || (md == d && __ldg(orig + (qi[start + mid] & kIdMask)) < key);
+                    if (before) lo = mid + 1;
+                    else hi = mid;
+                }
+                rank += lo;
+            }
+            start += n;
+        }
+        if (rank < K) out[rank] = key;
+    }
+}
+
 // Compute distances of the buffered fresh vertices bi[0..nb), keep the ones
 // that can still enter the queue, sort them and merge them. Returns the merge
 // position of the best survivor or L.
 template <int KIND, int ORDER, int CL, int STORE>
 __device__ uint32_t flush(const SearchArgs &a, const WarpMem &m, uint32_t nb, uint32_t *sz, uint32_t L,
                           bool filter, const Dist<KIND, CL, STORE> &D, int lane) {
+#if PANNS_WIDE_DIST
+    if constexpr (STORE == STORE_FP32) distances_wide<KIND, CL>(a, D.qv, m.bi, m.bd, nb, lane);
+    else D.distances(a, m.bi, m.bd, nb, lane);
+#else
     D.distances(a, m.bi, m.bd, nb, lane);
+#endif
     // Keep the survivors, in arrival order.
     const float bound = (filter && *sz >= L) ? m.qd[L - 1] : __int_as_float(0x7f800000);
     const bool any_bound = filter && *sz >= L;
@@ -849,15 +898,16 @@ __device__ void search_one(const SearchArgs &a, const WarpMem &m, uint32_t q, ui
 
     if (STORE != STORE_FP32) {
         // Re-rank the final L with the exact float32 distance (reference lane
-        // order) and order them by (distance, original id).
+        // order); the K best by (distance, original id) go out.
         Dist<KIND, CL, STORE_FP32> E;
         E.load(a, q, lane);
         E.distances(a, m.qi, m.qd, sz, lane);
-        rank_sort(m.qd, m.qi, sz, a.orig, lane);
+        rerank_output(m.qd, m.qi, sz, a.K, a.orig, a.out_ids + (size_t) q * a.K, lane);
+    } else {
+        // Results (original ids).
+        for (uint32_t i = lane; i < a.K; i += 32)
+            a.out_ids[(size_t) q * a.K + i] = __ldg(a.orig + (m.qi[i] & kIdMask));
     }
-    // Results (original ids) and counters.
-    for (uint32_t i = lane; i < a.K; i += 32)
-        a.out_ids[(size_t) q * a.K + i] = __ldg(a.orig + (m.qi[i] & kIdMask));
     if (lane == 0 && a.out_stats) a.out_stats[q] = make_uint4(n_dist, n_expand, n_edges, n_iter);
     // Clear the visited words this query set.
     if (dcount <= a.dirty_cap) {
