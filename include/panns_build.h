@@ -28,11 +28,22 @@ extern "C" {
 
 typedef struct panns_graph panns_graph;
 
+/* k-NN screen of the build: all pairs in float32 on CUDA cores keeping k + 8
+ * candidates per row, or by TF32 tensor-core GEMMs (cuBLAS) keeping k + 32;
+ * either way the candidates are ranked exactly in float64. AUTO: TF32 from
+ * 100,000 vectors on. */
+#define PANNS_SCREEN_AUTO 0u
+#define PANNS_SCREEN_FP32 1u
+#define PANNS_SCREEN_TF32 2u
+
 /* Build the graph of n row-major float32 vectors of width d (host pointer) on
  * GPU `device`; knn_k <= 128, 0 < R <= knn_k. *out is released with
  * panns_graph_free. */
 int panns_build_nsg(int device, const float *base, uint32_t n, uint32_t d, uint32_t knn_k, uint32_t R,
                     panns_graph **out);
+/* The same with the k-NN screen chosen (PANNS_SCREEN_*). */
+int panns_build_nsg_ex(int device, const float *base, uint32_t n, uint32_t d, uint32_t knn_k, uint32_t R,
+                       uint32_t screen, panns_graph **out);
 
 /* Sizes of a built graph (each pointer optional): vertices, largest degree,
  * entry vertex, total adjacency entries, in-edges added by the repair. */

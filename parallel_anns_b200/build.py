@@ -64,7 +64,7 @@ def build(force: bool = False, verbose: bool = False, extra=None) -> str:
         if p.wait() != 0:
             raise subprocess.CalledProcessError(p.returncode, cmd)
     link = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", SO + ".tmp"] + objs + [
-        "-lcudart"]
+        "-lcudart", "-lcublas"]
     subprocess.run(link, check=True, cwd=PKG)
     os.replace(SO + ".tmp", SO)
     return SO

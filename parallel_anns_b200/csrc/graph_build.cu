@@ -14,10 +14,13 @@
 //     in-edge from the first reached vertex of its k-NN list (else the entry),
 //     then everything it reaches is marked (index_nsg.cpp:638-718 plays this
 //     part with a DFS tree).
-// The k-NN search screens all pairs in float32 (||y||^2 - 2 x.y, tiled on
-// CUDA cores), keeps the C = k + 8 best per row, and ranks those by d64; the
-// result equals the exact k-NN unless a true neighbour falls outside the
-// float32 top C, which needs float32 rounding to move it past 8 others.
+// The k-NN search screens all pairs (||y||^2 - 2 x.y) either in float32 on CUDA
+// cores (tiled here, C = k + 8 candidates kept per row) or with TF32
+// tensor-core GEMMs (cuBLAS) folded tile by tile into the rows' lists (C = k +
+// 32), and ranks the C survivors by d64; the result equals the exact k-NN
+// unless a true neighbour falls outside the screen's top C, which needs the
+// screen's rounding to move it past 8 (float32) or 32 (TF32) others.
+#include <cublas_v2.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -60,6 +63,90 @@ __global__ void sqnorm32_kernel(const float *__restrict__ x, uint32_t n, uint32_
     float s = 0.f;
     for (uint32_t j = 0; j < d; ++j) s = fmaf(x[(size_t) r * d + j], x[(size_t) r * d + j], s);
     out[r] = s;
+}
+
+// Insert this warp's 32 candidates (dv, iv) (one per lane; +inf = none) into
+// the sorted list (rd, ri)[0..c) of capacity C, by (distance, id): each one
+// that beats the C-th in turn goes to its rank, the list shifting up by one.
+__device__ __forceinline__ void list_insert(float *rd, uint32_t *ri, uint32_t &c, uint32_t C, float dv, uint32_t iv,
+                                            int lane) {
+    const float thr_d = c == C ? rd[C - 1] : __int_as_float(0x7f800000);
+    const uint32_t thr_i = c == C ? ri[C - 1] : 0xffffffffu;
+    bool want = dv < thr_d || (dv == thr_d && iv < thr_i);
+    want = want && !(dv == __int_as_float(0x7f800000));
+    uint32_t bm = __ballot_sync(0xffffffffu, want);
+    while (bm) {
+        const int src = __ffs(bm) - 1;
+        bm &= bm - 1;
+        const float sd = __shfl_sync(0xffffffffu, dv, src);
+        const uint32_t si = __shfl_sync(0xffffffffu, iv, src);
+        // still better than the C-th after earlier inserts?
+        if (c == C && !(sd < rd[C - 1] || (sd == rd[C - 1] && si < ri[C - 1]))) continue;
+        // position = number of entries smaller than (sd, si)
+        uint32_t pos = 0;
+        for (uint32_t e0 = 0; e0 < c; e0 += 32) {
+            const uint32_t e = e0 + lane;
+            const bool less = e < c && (rd[e] < sd || (rd[e] == sd && ri[e] < si));
+            pos += __popc(__ballot_sync(0xffffffffu, less));
+        }
+        const uint32_t end = c < C ? c : C - 1;  // last index that moves
+        // shift [pos, end) up by one, from the top down in chunks of 32
+        for (int e0 = (int) end - 1; e0 >= (int) pos; e0 -= 32) {
+            const int e = e0 - lane;
+            float td = 0.f;
+            uint32_t ti = 0;
+            const bool mv = e >= (int) pos;
+            if (mv) {
+                td = rd[e];
+                ti = ri[e];
+            }
+            __syncwarp();
+            if (mv) {
+                rd[e + 1] = td;
+                ri[e + 1] = ti;
+            }
+            __syncwarp();
+        }
+        if (lane == 0) {
+            rd[pos] = sd;
+            ri[pos] = si;
+        }
+        __syncwarp();
+        if (c < C) ++c;
+    }
+}
+
+// Tensor-core screen, second half: G (nr x nc, row-major) holds -2 x_r . y_c
+// for rows r0.. and candidates c0..; one warp per row merges ||y_c||^2 + G
+// into the row's list (global ld / li / cnt, staged in shared memory).
+__global__ void __launch_bounds__(256) topk_tile_kernel(const float *__restrict__ G, uint32_t nr, uint32_t nc,
+                                                        uint32_t r0, uint32_t c0, const float *__restrict__ yn,
+                                                        uint32_t n, uint32_t C, float *__restrict__ gld,
+                                                        uint32_t *__restrict__ gli, uint32_t *__restrict__ gcnt) {
+    __shared__ float sd[8][kMaxC];
+    __shared__ uint32_t si[8][kMaxC];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t rr = blockIdx.x * 8 + w;
+    if (rr >= nr) return;
+    const uint32_t row = r0 + rr;
+    uint32_t c = gcnt[row];
+    for (uint32_t e = lane; e < c; e += 32) {
+        sd[w][e] = gld[(size_t) row * C + e];
+        si[w][e] = gli[(size_t) row * C + e];
+    }
+    __syncwarp();
+    const float *g = G + (size_t) rr * nc;
+    for (uint32_t j0 = 0; j0 < nc; j0 += 32) {
+        const uint32_t j = j0 + lane, col = c0 + j;
+        const bool ok = j < nc && col < n && col != row;
+        const float dv = ok ? g[j] + yn[col] : __int_as_float(0x7f800000);
+        list_insert(sd[w], si[w], c, C, dv, col, lane);
+    }
+    for (uint32_t e = lane; e < c; e += 32) {
+        gld[(size_t) row * C + e] = sd[w][e];
+        gli[(size_t) row * C + e] = si[w][e];
+    }
+    if (lane == 0) gcnt[row] = c;
 }
 
 // Float32 screen: for each of the kBQ rows of this block, the C candidates
@@ -128,57 +215,9 @@ __global__ void __launch_bounds__(256) screen_kernel(const float *__restrict__ x
         // Insert: rows 8w..8w+7 of this warp, each candidate that beats the
         // row's current C-th (distance, id).
         for (int r = warp * 8; r < warp * 8 + 8; ++r) {
-            float *rd = ld + r * C;
-            uint32_t *ri = li + r * C;
             uint32_t c = cnt[r];
-            for (int j0 = 0; j0 < kBV; j0 += 32) {
-                const float dv = D[r * (kBV + 1) + j0 + lane];
-                const uint32_t iv = v0 + j0 + lane;
-                const float thr_d = c == C ? rd[C - 1] : __int_as_float(0x7f800000);
-                const uint32_t thr_i = c == C ? ri[C - 1] : 0xffffffffu;
-                bool want = dv < thr_d || (dv == thr_d && iv < thr_i);
-                want = want && !(dv == __int_as_float(0x7f800000));
-                uint32_t bm = __ballot_sync(0xffffffffu, want);
-                while (bm) {
-                    const int src = __ffs(bm) - 1;
-                    bm &= bm - 1;
-                    const float sd = __shfl_sync(0xffffffffu, dv, src);
-                    const uint32_t si = __shfl_sync(0xffffffffu, iv, src);
-                    // still better than the C-th after earlier inserts?
-                    if (c == C && !(sd < rd[C - 1] || (sd == rd[C - 1] && si < ri[C - 1]))) continue;
-                    // position = number of entries smaller than (sd, si)
-                    uint32_t pos = 0;
-                    for (uint32_t e0 = 0; e0 < c; e0 += 32) {
-                        const uint32_t e = e0 + lane;
-                        const bool less = e < c && (rd[e] < sd || (rd[e] == sd && ri[e] < si));
-                        pos += __popc(__ballot_sync(0xffffffffu, less));
-                    }
-                    const uint32_t end = c < C ? c : C - 1;  // last index that moves
-                    // shift [pos, end) up by one, from the top down in chunks of 32
-                    for (int e0 = (int) end - 1; e0 >= (int) pos; e0 -= 32) {
-                        const int e = e0 - lane;
-                        float td = 0.f;
-                        uint32_t ti = 0;
-                        const bool mv = e >= (int) pos;
-                        if (mv) {
-                            td = rd[e];
-                            ti = ri[e];
-                        }
-                        __syncwarp();
-                        if (mv) {
-                            rd[e + 1] = td;
-                            ri[e + 1] = ti;
-                        }
-                        __syncwarp();
-                    }
-                    if (lane == 0) {
-                        rd[pos] = sd;
-                        ri[pos] = si;
-                    }
-                    __syncwarp();
-                    if (c < C) ++c;
-                }
-            }
+            for (int j0 = 0; j0 < kBV; j0 += 32)
+                list_insert(ld + r * C, li + r * C, c, C, D[r * (kBV + 1) + j0 + lane], v0 + j0 + lane, lane);
             if (lane == 0) cnt[r] = c;
             __syncwarp();
         }
@@ -295,13 +334,22 @@ extern "C" {
 
 int panns_build_nsg(int device, const float *base, uint32_t n, uint32_t d, uint32_t knn_k, uint32_t R,
                     panns_graph **out) {
+    return panns_build_nsg_ex(device, base, n, d, knn_k, R, PANNS_SCREEN_AUTO, out);
+}
+
+int panns_build_nsg_ex(int device, const float *base, uint32_t n, uint32_t d, uint32_t knn_k, uint32_t R,
+                       uint32_t screen, panns_graph **out) {
     if (!out || !base) return set_error(PANNS_EINVAL, "panns_build_nsg: NULL argument");
     *out = nullptr;
     if (n < 2 || d == 0) return set_error(PANNS_EINVAL, "panns_build_nsg: need n >= 2, d > 0");
     if (knn_k == 0 || knn_k >= n) return set_error(PANNS_EINVAL, "panns_build_nsg: need 0 < knn_k < n");
     if (knn_k + 8 > (uint32_t) kMaxC) return set_error(PANNS_EINVAL, "panns_build_nsg: knn_k > 128 is not supported");
     if (R == 0 || R > knn_k) return set_error(PANNS_EINVAL, "panns_build_nsg: need 0 < R <= knn_k");
-    const uint32_t k = knn_k, C = std::min(knn_k + 8, n - 1);
+    if (screen > PANNS_SCREEN_TF32) return set_error(PANNS_EINVAL, "panns_build_nsg: unknown screen");
+    if (screen == PANNS_SCREEN_AUTO) screen = n >= 100000 ? PANNS_SCREEN_TF32 : PANNS_SCREEN_FP32;
+    const bool tc = screen == PANNS_SCREEN_TF32;
+    const uint32_t k = knn_k;
+    const uint32_t C = std::min(std::min(knn_k + (tc ? 32u : 8u), (uint32_t) kMaxC), n - 1);
     GCU(cudaSetDevice(device));
     cudaStream_t s = nullptr;
     GCU(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
@@ -323,10 +371,46 @@ int panns_build_nsg(int device, const float *base, uint32_t n, uint32_t d, uint3
     GCU(dm.alloc(n));
     GCU(cudaMemcpyAsync(x.p, base, (size_t) n * d * 4, cudaMemcpyHostToDevice, s));
     sqnorm32_kernel<<<(n + 255) / 256, 256, 0, s>>>(x.p, n, d, xn.p);
-    const size_t smem = (size_t) (kBK * kBQ + kBK * kBV + kBQ * (kBV + 1)) * 4 + (size_t) kBQ * C * 8 + kBQ * 4;
-    GCU(cudaFuncSetAttribute(screen_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
-    screen_kernel<<<(n + kBQ - 1) / kBQ, 256, smem, s>>>(x.p, n, d, xn.p, C, cand.p);
-    GCU(cudaGetLastError());
+    if (!tc) {
+        const size_t smem = (size_t) (kBK * kBQ + kBK * kBV + kBQ * (kBV + 1)) * 4 + (size_t) kBQ * C * 8 + kBQ * 4;
+        GCU(cudaFuncSetAttribute(screen_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+        screen_kernel<<<(n + kBQ - 1) / kBQ, 256, smem, s>>>(x.p, n, d, xn.p, C, cand.p);
+        GCU(cudaGetLastError());
+    } else {
+        // -2 x.y for tiles of TR rows x TC candidates by TF32 tensor-core GEMMs
+        // (cuBLAS, a plain library GEMM), each folded into the rows' lists.
+        const uint32_t TR = std::min(n, 8192u), TC = std::min(n, 32768u);
+        Buf<float> G, gld;
+        Buf<uint32_t> gcnt;
+        GCU(G.alloc((size_t) TR * TC));
+        GCU(gld.alloc((size_t) n * C));
+        GCU(gcnt.alloc(n));
+        GCU(cudaMemsetAsync(gcnt.p, 0, n * 4ull, s));
+        cublasHandle_t hb = nullptr;
+        if (cublasCreate(&hb) != CUBLAS_STATUS_SUCCESS) return set_error(PANNS_ECUDA, "panns_build_nsg: cublasCreate failed");
+        struct HB {
+            cublasHandle_t h;
+            ~HB() { cublasDestroy(h); }
+        } hbg{hb};
+        if (cublasSetStream(hb, s) != CUBLAS_STATUS_SUCCESS)
+            return set_error(PANNS_ECUDA, "panns_build_nsg: cublasSetStream failed");
+        const float alpha = -2.f, beta = 0.f;
+        for (uint32_t r0 = 0; r0 < n; r0 += TR) {
+            const uint32_t nr = std::min(TR, n - r0);
+            for (uint32_t c0 = 0; c0 < n; c0 += TC) {
+                const uint32_t nc = std::min(TC, n - c0);
+                const cublasStatus_t st = cublasGemmEx(
+                    hb, CUBLAS_OP_T, CUBLAS_OP_N, (int) nc, (int) nr, (int) d, &alpha, x.p + (size_t) c0 * d, CUDA_R_32F,
+                    (int) d, x.p + (size_t) r0 * d, CUDA_R_32F, (int) d, &beta, G.p, CUDA_R_32F, (int) nc,
+                    CUBLAS_COMPUTE_32F_FAST_TF32, CUBLAS_GEMM_DEFAULT);
+                if (st != CUBLAS_STATUS_SUCCESS)
+                    return set_error(PANNS_ECUDA, "panns_build_nsg: cublasGemmEx failed (" + std::to_string((int) st) + ")");
+                topk_tile_kernel<<<(nr + 7) / 8, 256, 0, s>>>(G.p, nr, nc, r0, c0, xn.p, n, C, gld.p, cand.p, gcnt.p);
+                GCU(cudaGetLastError());
+            }
+        }
+        GCU(cudaStreamSynchronize(s));
+    }
     rerank_kernel<<<(n + 7) / 8, 256, 0, s>>>(x.p, n, d, cand.p, C, k, knn.p, knn_d.p);
     GCU(cudaGetLastError());
     prune_kernel<<<(n + 7) / 8, 256, 8 * R * 4, s>>>(x.p, n, d, knn.p, knn_d.p, k, R, pr.p, deg.p);

@@ -11,14 +11,18 @@ from . import native as N
 from .formats import NSGGraph
 
 
-def build_nsg(base: np.ndarray, R: int = 50, knn_k: int = 64, device: int = 0, with_knn: bool = False):
+SCREEN_AUTO, SCREEN_FP32, SCREEN_TF32 = 0, 1, 2
+
+
+def build_nsg(base: np.ndarray, R: int = 50, knn_k: int = 64, device: int = 0, with_knn: bool = False,
+              screen: int = SCREEN_AUTO):
     """Build the graph of ``base`` (n x d float32) on GPU ``device``.
     Returns an NSGGraph (and the n x knn_k k-NN ids if ``with_knn``)."""
     x = np.ascontiguousarray(base, dtype=np.float32)
     n, d = x.shape
     lib = N.load()
     g = ctypes.c_void_p()
-    N.check(lib.panns_build_nsg(device, N.ptr(x), n, d, knn_k, R, ctypes.byref(g)))
+    N.check(lib.panns_build_nsg_ex(device, N.ptr(x), n, d, knn_k, R, screen, ctypes.byref(g)))
     try:
         vals = [ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint64(), ctypes.c_uint32()]
         N.check(lib.panns_graph_info(g, *[ctypes.byref(v) for v in vals]))

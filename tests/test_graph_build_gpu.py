@@ -20,12 +20,14 @@ def same_graph(g, h):
             and np.array_equal(g.nbrs, h.nbrs))
 
 
+@pytest.mark.parametrize("screen", [1, 2])
 @pytest.mark.parametrize("n,d,k,R,seed", [(6000, 96, 64, 50, 1), (3000, 24, 32, 24, 2), (1500, 128, 40, 20, 3)])
-def test_gpu_graph_equals_oracle(n, d, k, R, seed):
+def test_gpu_graph_equals_oracle(n, d, k, R, seed, screen):
+    """Both k-NN screens (float32 CUDA cores, TF32 tensor cores) give the oracle's graph."""
     from parallel_anns_b200 import datasets as ds
     from parallel_anns_b200.graph import build_nsg
     x = ds.gaussian_mixture(n, d, seed=seed, means_seed=seed)
-    g, knn = build_nsg(x, R=R, knn_k=k, with_knn=True)
+    g, knn = build_nsg(x, R=R, knn_k=k, with_knn=True, screen=screen)
     og, oknn = O.build_nsg(x, k, R)
     bad = np.nonzero((knn != oknn).any(1))[0]
     assert bad.size == 0, f"k-NN rows differ: {bad[:10]}"
@@ -38,7 +40,9 @@ def test_gpu_graph_ties_and_repairs():
     a = rng.standard_normal((700, 32)).astype(np.float32)
     x = np.concatenate([a, a[:200], a[:40] + 40.0, a[:3] - 80.0]).astype(np.float32)
     g, knn = build_nsg(x, R=8, knn_k=16, with_knn=True)
+    g2 = build_nsg(x, R=8, knn_k=16, screen=2)
     og, oknn = O.build_nsg(x, 16, 8)
+    assert same_graph(g2, og)
     assert np.array_equal(knn, oknn)
     assert same_graph(g, og)
     assert g.repaired > 0
