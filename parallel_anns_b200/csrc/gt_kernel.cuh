@@ -43,16 +43,17 @@ __global__ void gt_tau_kernel(const float *__restrict__ base, int d, const float
 }
 
 // Grid: x = query tiles (fastest, so the tiles of one vertex range run
-// together and share it through L2), y = vertex tiles. 256 threads; thread
+// together and share it through L2), y = vertex tiles v_tile0 + blockIdx.y
+// (launched in slices of at most 65,535 tiles, the grid's y limit). 256 threads; thread
 // (ty, tx) owns queries 4*ty..4*ty+3 and vertices tx + 16*j, j < 8.
 __global__ void __launch_bounds__(256) gt_collect_kernel(const float *__restrict__ base, uint32_t n, int d,
                                                          const float *__restrict__ queries, uint32_t nq,
                                                          const double *__restrict__ tau, uint32_t cap,
                                                          uint32_t *__restrict__ cnt, double *__restrict__ cand_d,
-                                                         uint32_t *__restrict__ cand_i) {
+                                                         uint32_t *__restrict__ cand_i, uint32_t v_tile0) {
     __shared__ double sq[kGtK][kGtQ];
     __shared__ double sv[kGtK][kGtV];
-    const uint32_t q0 = blockIdx.x * kGtQ, v0 = blockIdx.y * kGtV;
+    const uint32_t q0 = blockIdx.x * kGtQ, v0 = (blockIdx.y + v_tile0) * kGtV;
     const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
     double acc[4][8];
 #pragma unroll

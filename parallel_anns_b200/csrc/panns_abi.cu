@@ -1146,9 +1146,12 @@ int panns_ground_truth(panns_index *h, const float *queries, uint32_t nq, uint32
         CU(cd.ensure((size_t) nq * cap));
         CU(ci.ensure((size_t) nq * cap));
         CU(cudaMemsetAsync(dcnt.p, 0, nq * 4ull, h->stream));
-        dim3 grid((nq + kGtQ - 1) / kGtQ, (h->n + kGtV - 1) / kGtV);
-        gt_collect_kernel<<<grid, 256, 0, h->stream>>>(h->base_raw.p, h->n, (int) h->d, dq.p, nq, dtau.p, cap,
-                                                      dcnt.p, cd.p, ci.p);
+        const uint32_t vt = (h->n + kGtV - 1) / kGtV;
+        for (uint32_t t0 = 0; t0 < vt; t0 += 65535u) {
+            dim3 grid((nq + kGtQ - 1) / kGtQ, std::min(65535u, vt - t0));
+            gt_collect_kernel<<<grid, 256, 0, h->stream>>>(h->base_raw.p, h->n, (int) h->d, dq.p, nq, dtau.p, cap,
+                                                           dcnt.p, cd.p, ci.p, t0);
+        }
         CU(cudaGetLastError());
         CU(cudaMemcpyAsync(cnt.data(), dcnt.p, nq * 4ull, cudaMemcpyDeviceToHost, h->stream));
         CU(cudaStreamSynchronize(h->stream));
