@@ -378,10 +378,11 @@ def bench_ours(args):
     if os.path.exists(tp):
         try:
             with open(tp) as f:
-                tj = json.load(f)
-            if (tj.get("L"), tj.get("M"), tj.get("n"), tj.get("storage"), tj.get("learned")) == (
-                    L, M, args.n, names[store], head.learned is not None):
-                traffic = tj["dram_bytes_per_query"] * nq
+                entries = json.load(f)
+            for tj in entries if isinstance(entries, list) else [entries]:
+                if (tj.get("L"), tj.get("M"), tj.get("n"), tj.get("storage"), tj.get("learned")) == (
+                        L, M, args.n, names[store], head.learned is not None):
+                    traffic = tj["dram_bytes_per_query"] * nq
         except Exception:
             traffic = None
     p_alg = (p_tot["n_dist"] * (4 * d + 4) + 4 * p_tot["n_edges"]) / steps + nq * (4 * d + 4 * K)

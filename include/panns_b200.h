@@ -84,8 +84,9 @@ typedef struct {
                                 EFANNA: with the first L_query[i] of its L init ids. NULL = L
                                 for every query. No counterpart in the reference (one L per
                                 call, PSS.cpp:1218). */
-    uint32_t blocks_per_sm;  /* resident blocks per SM (0 = as many as fit); fewer leave more of
-                                the SM's L1 / shared array to L1, which caches gathered rows */
+    uint32_t blocks_per_sm;  /* resident blocks per SM; fewer leave more of the SM's L1 / shared
+                                array to L1, which caches gathered rows. 0 = as many as fit,
+                                but no more than fit in 196 KB of shared memory */
     uint32_t warps_per_query; /* 0 or 1: one warp per query (warps_per_block queries per block);
                                  2 or 4: that many warps share each query's steps (one query per
                                  block; NSG_SEQ, TOP_M, PSS_V5 at T = 1, FP32 storage), for small

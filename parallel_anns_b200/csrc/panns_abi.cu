@@ -798,16 +798,29 @@ static int launch_search(panns_index *h, const panns_search_params *p, float *d_
                                           " for this kernel");
     }
     CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
-    // The L1 / shared-memory split: by default the driver's (enough shared
-    // memory for the most resident blocks); with blocks_per_sm, just enough
-    // shared memory for that many blocks, the rest of the array left to L1,
-    // which caches the gathered rows.
+    // The L1 / shared-memory split: the driver's first (enough shared memory
+    // for the most resident blocks); with a block count (blocks_per_sm, or the
+    // default below), just enough shared memory for that many blocks, the rest
+    // of the array left to L1, which caches the gathered rows.
     CU(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
                             carveout_percent(smem, p->blocks_per_sm)));
     int per_sm = 0;
     CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (int) wpb * 32, smem));
     if (per_sm < 1) return fail(PANNS_EINVAL, "search: L too large for shared memory");
-    if (p->blocks_per_sm) per_sm = std::min(per_sm, (int) p->blocks_per_sm);
+    uint32_t bps = p->blocks_per_sm;
+    if (!bps) {
+        // As many resident blocks as fit, unless that takes the whole 228 KB
+        // array as shared memory (28 KB of L1 left): then as many as fit in
+        // 196 KB. Measured on the 1M set: L = 448, 8.9 ms (5 blocks) against
+        // 10.0 ms (6 blocks); L = 512 with 2-warp blocks, 9.8 ms (10) against 11.0 (12).
+        const size_t per_block = smem + 1024;
+        const int fit = (int) ((196u << 10) / per_block);
+        if ((size_t) per_sm * per_block > (196u << 10) && fit >= 1) bps = (uint32_t) fit;
+    }
+    if (bps) {
+        CU(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, carveout_percent(smem, bps)));
+        per_sm = std::min(per_sm, (int) bps);
+    }
     uint32_t blocks = (uint32_t) per_sm * (uint32_t) h->num_sms;
     const uint32_t need_blocks = (nq + qpb - 1) / qpb;
     blocks = std::max(1u, std::min(blocks, need_blocks));
