@@ -322,31 +322,34 @@ def bench_ours(args):
     # Batch sizes 1, 64 and 1000 through the asynchronous device-pointer entry
     # point with the CUDA-graph-captured launch, batches back to back on one
     # stream (device time from the first launch to the last result).
-    # Per batch size the warps per query is tuned too (1, 2, 4; several warps
-    # only for the plain FP32 search), at the head's L and M.
+    # Per batch size the warps per query is tuned too (1, 2, 4), at the head's L and M.
     batching = {}
     qd = torch.from_numpy(qs).cuda()
     stream = torch.cuda.Stream()
     for B, nb in ((1, 300), (64, 60), (1000, 10)):
         outb = torch.empty((B, K), dtype=torch.int32, device="cuda")
         best_b, tried = None, {}
-        wpq_options = [1]
-        if head.storage == N.STORE_FP32 and head.learned is None:
-            wpq_options += [2, 4]
-        for wq in wpq_options:
-            kwb = dict(kw, flags=kw["flags"] | N.FLAG_CUDA_GRAPH, warps_per_query=wq)
+        # the head's own configuration (one warp per query), then the plain
+        # FP32 search at the head's L and M with 2 and 4 warps per query (the
+        # several-warps kernel searches the float32 rows, without the network)
+        options = [(1, ixh, dict(kw, flags=kw["flags"] | N.FLAG_CUDA_GRAPH))]
+        for wq in (2, 4):
+            options.append((wq, handles[N.STORE_FP32],
+                            dict(kw, storage=N.STORE_FP32, flags=N.FLAG_CUDA_GRAPH, warps_per_query=wq)))
+        for wq, ixb, kwb in options:
             for i in range(3):
-                ixh.search_device(qd[i * B:(i + 1) * B], outb, K=K, stream=stream, **kwb)
+                ixb.search_device(qd[i * B:(i + 1) * B], outb, K=K, stream=stream, **kwb)
             stream.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
             for i in range(nb):
                 s0 = (i * B) % (nq - B + 1)
-                ixh.search_device(qd[s0:s0 + B], outb, K=K, stream=stream, **kwb)
+                ixb.search_device(qd[s0:s0 + B], outb, K=K, stream=stream, **kwb)
             e1.record(stream)
             stream.synchronize()
             ms = e0.elapsed_time(e1)
-            r_ = {"qps": round(nb * B / (ms / 1e3), 1), "ms_per_batch": round(ms / nb, 4), "warps_per_query": wq}
+            r_ = {"qps": round(nb * B / (ms / 1e3), 1), "ms_per_batch": round(ms / nb, 4), "warps_per_query": wq,
+                  "storage": names[kwb["storage"]]}
             tried[str(wq)] = r_["qps"]
             if best_b is None or r_["qps"] > best_b["qps"]:
                 best_b = r_
