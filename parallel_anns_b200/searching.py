@@ -125,8 +125,9 @@ class Index:
     def search(self, queries: np.ndarray | None = None, *, K=100, L=100, mode=N.MODE_NSG_SEQ,
                distance=N.DIST_NORM_IP, M=1, T=1, L_local=0, X=1, init_ids=None,
                q_begin=0, nq=None, warps_per_block=0, storage=N.STORE_FP32, flags=0, L_query=None,
-               blocks_per_sm=0, warps_per_query=0):
-        """Search a batch. With ``queries`` None the loaded queries
+               blocks_per_sm=0, warps_per_query=0, out=None):
+        """Search a batch. ``out`` (optional): a C-contiguous nq x K uint32
+        array to write the ids into (e.g. a view of pinned host memory). With ``queries`` None the loaded queries
         [q_begin, q_begin + nq) are used. ``L_query``: optional per-query
         queue lengths (K <= L_query[i] <= L). Returns (ids [nq x K], stats dict)."""
         if L_query is not None:
@@ -139,13 +140,13 @@ class Index:
             ii = np.ascontiguousarray(init_ids, dtype=np.uint32)
         if queries is None:
             nq = self.nq - q_begin if nq is None else nq
-            out = np.empty((nq, K), dtype=np.uint32)
+            out = np.empty((nq, K), dtype=np.uint32) if out is None else out
             N.check(self._lib.panns_search(self._h, ctypes.byref(p), N.ptr(ii) if ii is not None else None,
                                            q_begin, nq, N.ptr(out), ctypes.byref(st)))
         else:
             queries = np.ascontiguousarray(queries, dtype=np.float32)
             nq = queries.shape[0]
-            out = np.empty((nq, K), dtype=np.uint32)
+            out = np.empty((nq, K), dtype=np.uint32) if out is None else out
             N.check(self._lib.panns_search_host(self._h, ctypes.byref(p), N.ptr(queries), nq,
                                                 N.ptr(ii) if ii is not None else None, N.ptr(out),
                                                 ctypes.byref(st)))
