@@ -183,7 +183,7 @@ def bench_ours(args):
     barrier = ranks.barrier
     max_over_ranks = ranks.max
 
-    spec = workloads.spec_batched_fp32_1m(n=args.n, nq=args.nq * world)
+    spec = workloads.SPECS[args.workload](n=args.n, nq=args.nq * world)
     fixed = bool(args.L and args.M)  # a given operating point: no tuning set, no autotuning
     if rank == 0:
         W = workloads.build(spec, device=f"cuda:{local}", log=log)
@@ -412,8 +412,7 @@ def bench_ours(args):
             "steps": steps, "warmup": args.warmup,
             "ms_per_step": round(kernel_ms_max / steps, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": names[store], "data": "synthetic",
-            "config": {"workload": "batched search, 1M x 96d mixture64 (sigma 0.3, unit norm), "
-                                   "NSG-style graph R=50, 10k queries per GPU, K=100",
+            "config": {"workload": "batched search, " + workloads.describe(spec) + " (per GPU)",
                        "n": args.n, "d": d, "queries_per_gpu": nq, "K": K, "L": L, "M": M,
                        "warps_per_block": head.warps_per_block, "warps_per_query": head.warps_per_query,
                        "blocks_per_sm": head.blocks_per_sm,
@@ -428,7 +427,8 @@ def bench_ours(args):
                        "operating_point": ("fixed by --L/--M" if fixed else
                                            "autotuned on 10k held-out tuning queries (another seed); "
                                            "recall and speed measured on the 10k evaluation queries"),
-                       "l2": "inputs larger than L2 (384 MB base) and a 256 MB L2 flush before each step",
+                       "l2": f"inputs larger than L2 ({args.n * d * 4 >> 20} MB base) and a 256 MB L2 flush "
+                             "before each step",
                        "autotune": choices["tables"]},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
@@ -500,7 +500,7 @@ def bench_reference(args):
         print(json.dumps({"impl": "reference", "unavailable":
                           "reference checker binaries were not built (oracle/_ref/ref_pss missing)"}))
         return
-    spec = workloads.spec_batched_fp32_1m(n=args.n, nq=args.nq)
+    spec = workloads.SPECS[args.workload](n=args.n, nq=args.nq)
     dev = f"cuda:{local}" if torch.cuda.is_available() else "cpu"
     W = workloads.build(spec, device=dev, log=log)
     T = nproc()
@@ -536,9 +536,8 @@ def bench_reference(args):
             "ms_per_step": round(1e3 * sum(times) / len(times), 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": "batched FP32 search, 1M x 96d mixture64 (sigma 0.3, unit norm), "
-                                   "NSG-style graph R=50, 10k queries per GPU, K=100",
-                       "n": args.n, "d": 96, "K": 100, "L": L, "T": T, "X": X, "mode": mode_name,
+            "config": {"workload": "batched search, " + workloads.describe(spec),
+                       "n": args.n, "d": spec["d"], "K": 100, "L": L, "T": T, "X": X, "mode": mode_name,
                        "recall100": r["recall100"], "queries_per_step": sample},
             "cpu_baseline": {"value": round(value, 1), "unit": UNIT, "cores": T, "kind": "reference",
                              "sample": f"{sample} queries per step, {mode_name}, L_master=L_local={L}, "
@@ -563,6 +562,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="leave the learned entry network out")
     ap.add_argument("--wpb", type=int, default=2, help="warps per block with a fixed --L and --M")
+    ap.add_argument("--workload", default="mixture_1m_d96", choices=["mixture_1m_d96", "u8_1m_d128"],
+                    help="mixture_1m_d96: the batched-FP32 config (default); u8_1m_d128: the "
+                         "reduced-precision config's integer-valued d = 128 variant (R = 64)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

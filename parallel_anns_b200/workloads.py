@@ -31,6 +31,35 @@ def spec_batched_fp32_1m(n=1_000_000, nq=10_000, d=96):
             "gt_k": 100}
 
 
+def spec_u8_1m_d128(n=1_000_000, nq=10_000):
+    """The reduced-precision config's integer variant: d = 128, components
+    uniform in 0..255 stored as uint8 and cast to float32, R = 64."""
+    return {"name": f"u8cube_n{n}_d128_q{nq}_R64", "kind": "uint8", "n": n, "d": 128, "nq": nq, "R": 64,
+            "knn_k": 64, "base_seed": 1002, "query_seed": 2002, "gt_k": 100}
+
+
+SPECS = {"mixture_1m_d96": spec_batched_fp32_1m, "u8_1m_d128": spec_u8_1m_d128}
+
+
+def describe(spec) -> str:
+    """One line naming the workload with its sizes."""
+    if spec.get("kind") == "uint8":
+        data = f"{spec['n'] // 1000}k x {spec['d']}d integer-valued (uniform 0..255, uint8 cast to float32)"
+    else:
+        data = (f"{spec['n'] // 1000}k x {spec['d']}d mixture{spec['components']} "
+                f"(sigma {spec['sigma']}, unit norm)")
+    return f"{data}, NSG-style graph R={spec['R']}, {spec['nq']} queries, K={spec['gt_k']}"
+
+
+def vectors(spec, count, seed):
+    """`count` vectors of the workload's distribution (queries use the base's
+    mixture means)."""
+    if spec.get("kind") == "uint8":
+        return ds.uint8_cube(count, spec["d"], seed=seed)
+    return ds.gaussian_mixture(count, spec["d"], spec["components"], spec["sigma"], seed=seed,
+                               means_seed=spec["base_seed"])
+
+
 def paths(spec):
     root = os.path.join(CACHE, spec["name"])
     return {k: os.path.join(root, v) for k, v in
@@ -48,10 +77,8 @@ def build(spec, device=None, log=print):
             return load(spec)
     os.makedirs(p["root"], exist_ok=True)
     t0 = time.time()
-    base = ds.gaussian_mixture(spec["n"], spec["d"], spec["components"], spec["sigma"],
-                               seed=spec["base_seed"], means_seed=spec["base_seed"])
-    q = ds.gaussian_mixture(spec["nq"], spec["d"], spec["components"], spec["sigma"],
-                            seed=spec["query_seed"], means_seed=spec["base_seed"])
+    base = vectors(spec, spec["n"], spec["base_seed"])
+    q = vectors(spec, spec["nq"], spec["query_seed"])
     t1 = time.time()
     g = build_graph(base, spec, device)
     t2 = time.time()
@@ -110,8 +137,7 @@ def tuning_set(spec, W, n_tune=10_000, device=None):
     if os.path.exists(path):
         z = np.load(path)
         return z["q"], z["gt"]
-    q = ds.gaussian_mixture(n_tune, spec["d"], spec["components"], spec["sigma"],
-                            seed=spec["query_seed"] + 1, means_seed=spec["base_seed"])
+    q = vectors(spec, n_tune, spec["query_seed"] + 1)
     gt, _ = ground_truth(W["base"], W["graph"], q, spec["gt_k"], device)
     np.savez(path, q=q, gt=gt)
     return q, gt
@@ -122,8 +148,7 @@ def learned_model(spec, index, n_train=200_000, R=1024, log=print):
     held-out queries (cached next to the workload)."""
     from . import learned as LE
     cache = os.path.join(paths(spec)["root"], f"learned_R{R}_t{n_train}.npz")
-    train_q = ds.gaussian_mixture(n_train, spec["d"], spec["components"], spec["sigma"],
-                                  seed=spec["base_seed"] + 2000, means_seed=spec["base_seed"])
+    train_q = vectors(spec, n_train, spec["base_seed"] + 2000)
     t0 = time.time()
     m = LE.build_model(index, train_q, R=R, K=spec["gt_k"], M=8, L_ref=1000, T=10, epochs=10, batch=1024,
                        lr=2e-3, lam=1.0, seed=0, kmeans_iters=15, cache=cache, log=log)
