@@ -83,7 +83,7 @@ def tune(index, queries, gt, *, K=100, target=0.95, storages=(N.STORE_FP32,), Ms
             for M in Ms:
                 flags = N.FLAG_LEARNED if opt is not None else 0
                 mode = N.MODE_NSG_SEQ if M == 1 else N.MODE_TOP_M
-                kw = dict(M=M, mode=mode, storage=store, flags=flags, warps_per_block=4)
+                kw = dict(M=M, mode=mode, storage=store, flags=flags, warps_per_block=0)
                 rec_at = {}
 
                 def rec(L):
@@ -110,7 +110,12 @@ def tune(index, queries, gt, *, K=100, target=0.95, storages=(N.STORE_FP32,), Ms
                     # blocks_per_sm counts blocks of w warps: keep the warps per SM comparable
                     b = bps * 4 // w if bps else 0
                     kw2 = dict(kw, warps_per_block=w, blocks_per_sm=b, warps_per_query=wq)
-                    _, ms = _time(index, queries, K, dict(kw2, L=L), reps)
+                    try:
+                        _, ms = _time(index, queries, K, dict(kw2, L=L), reps)
+                    except N.PannsError as e:  # a block shape that does not fit this L
+                        if e.code != -1:
+                            raise
+                        continue
                     row = {"storage": store, "M": M, "learned": opt, "L": L, "warps_per_block": w,
                            "blocks_per_sm": b, "warps_per_query": wq, "recall": rec(L), "kernel_ms": ms}
                     table.append(row)

@@ -785,6 +785,9 @@ static int launch_search(panns_index *h, const panns_search_params *p, float *d_
     if (pss && !p->warps_per_block) {
         while (wpb > 1 && wpb * per_warp > (100u << 10)) --wpb;
     }
+    if (wpq == 1 && !p->warps_per_block) {  // default block shape: as many warps as fit (long queues)
+        while (wpb > 1 && wpb * per_warp > (227u << 10)) --wpb;
+    }
     if (per_warp > (227u << 10))
         return fail(PANNS_EINVAL, "search: the queues (L, T x L_local) do not fit in shared memory");
     const size_t smem = wpq > 1 ? (size_t) block_smem_bytes(qcap, wpq) : (size_t) wpb * per_warp;
