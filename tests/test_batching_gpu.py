@@ -183,3 +183,14 @@ def test_several_warps_per_query_dimensions(N_lib, d):
             ref, st = ix.search(K=50, L=120, mode=1, M=4, distance=dist)
             got, st2 = ix.search(K=50, L=120, mode=1, M=4, distance=dist, warps_per_query=2)
             assert np.array_equal(got, ref) and st["n_dist"] == st2["n_dist"]
+
+
+def test_long_queue_default_block_shape(setup):
+    """L = 8192: four one-warp queues do not fit a block's shared memory, so the
+    default block shape shrinks (an explicit 4 is rejected); ids equal the oracle's."""
+    ix, N, base, q, g = setup
+    with pytest.raises(N.PannsError):
+        ix.search(q[:8], K=100, L=8192, mode=N.MODE_TOP_M, M=8, warps_per_block=4)
+    got, _ = ix.search(q[:8], K=100, L=8192, mode=N.MODE_TOP_M, M=8)
+    ref, _ = O.search_top_m(base, O.Graph.from_nsg(g), q[:8], 100, 8192, 8)
+    assert np.array_equal(got, ref)
