@@ -335,11 +335,13 @@ def bench_ours(args):
     for B, nb in ((1, 300), (64, 60), (1000, 10)):
         outb = torch.empty((B, K), dtype=torch.int32, device="cuda")
         best_b, tried = None, {}
-        # the head's own configuration (one warp per query), then the plain
-        # FP32 search at the head's L and M with 2 and 4 warps per query (the
-        # several-warps kernel searches the float32 rows, without the network)
-        options = [(1, ixh, dict(kw, flags=kw["flags"] | N.FLAG_CUDA_GRAPH))]
-        for wq in (2, 4):
+        # the head's own configuration, then the plain FP32 search at the
+        # head's L and M with 1, 2 and 4 warps per query (the several-warps
+        # kernel searches the float32 rows, without the network)
+        options = [(head.warps_per_query, ixh, dict(kw, flags=kw["flags"] | N.FLAG_CUDA_GRAPH))]
+        for wq in (1, 2, 4):
+            if wq == head.warps_per_query and head.storage == N.STORE_FP32 and head.learned is None:
+                continue  # the head itself
             options.append((wq, handles[N.STORE_FP32],
                             dict(kw, storage=N.STORE_FP32, flags=N.FLAG_CUDA_GRAPH, warps_per_query=wq)))
         for wq, ixb, kwb in options:
@@ -356,7 +358,7 @@ def bench_ours(args):
             ms = e0.elapsed_time(e1)
             r_ = {"qps": round(nb * B / (ms / 1e3), 1), "ms_per_batch": round(ms / nb, 4), "warps_per_query": wq,
                   "storage": names[kwb["storage"]]}
-            tried[str(wq)] = r_["qps"]
+            tried[f"{wq}/{names[kwb['storage']]}"] = r_["qps"]
             if best_b is None or r_["qps"] > best_b["qps"]:
                 best_b = r_
         batching[str(B)] = dict(best_b, qps_by_warps_per_query=tried)
