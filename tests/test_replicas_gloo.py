@@ -21,7 +21,9 @@ def _worker(rank, world, port, q):
     ranks.barrier()
     mx = ranks.max(1.5 + r)
     choice = ranks.broadcast_ints([7 + r, 400, 8], 0)
-    q.put((r, w, lr, sl.start, sl.stop, mx, choice))
+    # the bench's operating point (autotuner choice, a JSON object) from rank 0
+    obj = ranks.broadcast_json({"head": {"storage": 2, "L": 384, "learned": None}, "rank": r} if r == 0 else None, 0)
+    q.put((r, w, lr, sl.start, sl.stop, mx, choice, obj))
     dist.destroy_process_group()
 
 
@@ -40,8 +42,9 @@ def test_two_gloo_ranks():
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
-    (r0, w0, l0, a0, b0, m0, c0), (r1, w1, l1, a1, b1, m1, c1) = out
+    (r0, w0, l0, a0, b0, m0, c0, o0), (r1, w1, l1, a1, b1, m1, c1, o1) = out
     assert (r0, r1, w0, w1) == (0, 1, 2, 2)
     assert (a0, b0, a1, b1) == (0, 100, 100, 200)
     assert m0 == m1 == 2.5
     assert c0 == c1 == [7, 400, 8]
+    assert o0 == o1 == {"head": {"storage": 2, "L": 384, "learned": None}, "rank": 0}
