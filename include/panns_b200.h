@@ -73,7 +73,8 @@ typedef struct {
     uint32_t T;           /* PSS_V5: number of queues (workers + master, >= 1) */
     uint32_t L_local;     /* PSS_V5: worker queue capacity (0 = L) */
     uint32_t X;           /* PSS_V5: expansions per worker per stage (>= 1) */
-    uint32_t warps_per_block; /* warps (queries in flight) per block, <= 4; 0 = 4 */
+    uint32_t warps_per_block; /* warps (queries in flight) per block, <= 4; 0 = 4, fewer when four
+                                 queues of L do not fit one block's shared memory */
     uint32_t storage;     /* panns_storage the search distances use: FP32 (exact), or
                              the reduced copy built by panns_set_base (NSG_SEQ / TOP_M
                              only; the final L are re-ranked in exact FP32) */
