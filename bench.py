@@ -335,15 +335,17 @@ def bench_ours(args):
     for B, nb in ((1, 300), (64, 60), (1000, 10)):
         outb = torch.empty((B, K), dtype=torch.int32, device="cuda")
         best_b, tried = None, {}
-        # the head's own configuration, then the plain FP32 search at the
-        # head's L and M with 1, 2 and 4 warps per query (the several-warps
-        # kernel searches the float32 rows, without the network)
+        # the head's own configuration, then the head's storage, L and M
+        # without the learned prologue, with 1, 2 and 4 warps per query
         options = [(head.warps_per_query, ixh, dict(kw, flags=kw["flags"] | N.FLAG_CUDA_GRAPH))]
         for wq in (1, 2, 4):
-            if wq == head.warps_per_query and head.storage == N.STORE_FP32 and head.learned is None:
+            if wq == head.warps_per_query and head.learned is None:
                 continue  # the head itself
-            options.append((wq, handles[N.STORE_FP32],
-                            dict(kw, storage=N.STORE_FP32, flags=N.FLAG_CUDA_GRAPH, warps_per_query=wq)))
+            options.append((wq, ixh, dict(kw, flags=N.FLAG_CUDA_GRAPH, warps_per_query=wq)))
+        if head.storage != N.STORE_FP32:  # and the float32 rows with several warps
+            for wq in (2, 4):
+                options.append((wq, handles[N.STORE_FP32],
+                                dict(kw, storage=N.STORE_FP32, flags=N.FLAG_CUDA_GRAPH, warps_per_query=wq)))
         for wq, ixb, kwb in options:
             for i in range(3):
                 ixb.search_device(qd[i * B:(i + 1) * B], outb, K=K, stream=stream, **kwb)

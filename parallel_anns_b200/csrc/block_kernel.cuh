@@ -1,6 +1,7 @@
-// Several warps per query: the same exact search as search_kernel (PANNS
-// order, float32 distances), for small batches where one warp per query
-// leaves the GPU idle and every query pays the whole serial latency.
+// Several warps per query: the same search as search_kernel (PANNS order; the
+// float32 rows, or a BF16 / FP8 copy with the exact float32 re-rank of the
+// final L), for small batches where one warp per query leaves the GPU idle and
+// every query pays the whole serial latency, and for long queues.
 //
 // One block of W warps runs one query at a time (work-stealing counter across
 // blocks). The queue lives in the block's shared memory. A search step is:
@@ -49,7 +50,7 @@ __device__ __forceinline__ uint32_t list_rank(const float *d, const uint32_t *k,
     return lo;
 }
 
-template <int KIND, int CL, int W>
+template <int KIND, int CL, int W, int STORE>
 __device__ void block_search_one(const SearchArgs &a, uint32_t q, uint8_t *smem, uint32_t *vis, uint32_t *dirty) {
     constexpr int T = W * 32;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
@@ -73,7 +74,7 @@ __device__ void block_search_one(const SearchArgs &a, uint32_t q, uint8_t *smem,
     uint32_t *pre = preAll + w * 64;
 
     const uint32_t L = a.Lq ? __ldg(a.Lq + q) : a.L;
-    Dist<KIND, CL, STORE_FP32> D;
+    Dist<KIND, CL, STORE> D;
     D.load(a, q, lane);
     if (tid == 0) {
         ctl[BC_SZ] = 0;
@@ -156,7 +157,8 @@ __device__ void block_search_one(const SearchArgs &a, uint32_t q, uint8_t *smem,
     // Distances, filter against the queue's L-th (bound), keys, sort; leaves
     // the warp's survivor count in ctl[BC_SEG + w].
     auto finish_list = [&](uint32_t nb, bool filter) {
-        distances_wide<KIND, CL>(a, D.qv, bi, bd, nb, lane);
+        if constexpr (STORE == STORE_FP32) distances_wide<KIND, CL>(a, D.qv, bi, bd, nb, lane);
+        else D.distances(a, bi, bd, nb, lane);
         if (lane == 0 && nb) atomicAdd(&ctl[BC_DIST], nb);
         const uint32_t sz = ctl[BC_SZ];
         const bool any_bound = filter && sz >= L;
@@ -352,7 +354,18 @@ __device__ void block_search_one(const SearchArgs &a, uint32_t q, uint8_t *smem,
         __syncthreads();
     }
 
-    for (uint32_t i = tid; i < a.K; i += T) a.out_ids[(size_t) q * a.K + i] = __ldg(a.orig + (qi[i] & kIdMask));
+    if constexpr (STORE != STORE_FP32) {
+        // Re-rank the final L in exact float32 (warp 0), as search_kernel does.
+        if (w == 0) {
+            Dist<KIND, CL, STORE_FP32> E;
+            E.load(a, q, lane);
+            const uint32_t sz = ctl[BC_SZ];
+            E.distances(a, qi, qd, sz, lane);
+            rerank_output(qd, qi, sz, a.K, a.orig, a.out_ids + (size_t) q * a.K, lane);
+        }
+    } else {
+        for (uint32_t i = tid; i < a.K; i += T) a.out_ids[(size_t) q * a.K + i] = __ldg(a.orig + (qi[i] & kIdMask));
+    }
     if (tid == 0 && a.out_stats) a.out_stats[q] = make_uint4(ctl[BC_DIST], n_expand, ctl[BC_EDGES], n_iter);
     const uint32_t dcount = ctl[BC_DIRTY];
     if (dcount <= a.dirty_cap) {
@@ -363,7 +376,7 @@ __device__ void block_search_one(const SearchArgs &a, uint32_t q, uint8_t *smem,
     __syncthreads();
 }
 
-template <int KIND, int CL, int W>
+template <int KIND, int CL, int W, int STORE>
 __global__ void __launch_bounds__(W * 32) search_block_kernel(SearchArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
     const uint32_t slot = blockIdx.x;
@@ -376,7 +389,7 @@ __global__ void __launch_bounds__(W * 32) search_block_kernel(SearchArgs a) {
         const uint32_t q = ctl[BC_Q];
         __syncthreads();
         if (q >= a.nq) break;
-        block_search_one<KIND, CL, W>(a, q, smem, vis, dirty);
+        block_search_one<KIND, CL, W, STORE>(a, q, smem, vis, dirty);
     }
 }
 

@@ -27,9 +27,17 @@ inline const void *search_kernel_ptr(uint32_t kind, uint32_t order, int CL, uint
     if (store == 2) return search_kernel_ptr_fp8(kind, order, CL);
     return kind == 0 ? search_kernel_ptr_fp32_ip(kind, order, CL) : search_kernel_ptr_fp32_l2(kind, order, CL);
 }
-// search_block_kernel<KIND, CL, W> (block_kernel.cuh), W warps per query;
-// nullptr if not built (W other than 2 and 4).
-const void *search_block_kernel_ptr(uint32_t kind, int CL, uint32_t W);
+// search_block_kernel<KIND, CL, W, STORE> (block_kernel.cuh), W warps per
+// query; nullptr if not built (W other than 2 and 4).
+const void *search_block_kernel_ptr_fp32(uint32_t kind, int CL, uint32_t W);
+const void *search_block_kernel_ptr_bf16(uint32_t kind, int CL, uint32_t W);
+const void *search_block_kernel_ptr_fp8(uint32_t kind, int CL, uint32_t W);
+
+inline const void *search_block_kernel_ptr(uint32_t kind, int CL, uint32_t W, uint32_t store) {
+    if (store == 1) return search_block_kernel_ptr_bf16(kind, CL, W);
+    if (store == 2) return search_block_kernel_ptr_fp8(kind, CL, W);
+    return search_block_kernel_ptr_fp32(kind, CL, W);
+}
 // pss_kernel<KIND, CL> (pss_kernel.cuh); nullptr if not built.
 const void *pss_kernel_ptr(uint32_t kind, int CL);
 

@@ -649,9 +649,9 @@ int check_params(panns_index *h, const panns_search_params *p) {
             return fail(PANNS_EINVAL, "search: warps_per_query must be 0, 1, 2 or 4");
         const bool ok = p->mode == PANNS_MODE_NSG_SEQ || p->mode == PANNS_MODE_TOP_M ||
                         (p->mode == PANNS_MODE_PSS_V5 && p->T == 1);
-        if (!ok || p->storage != PANNS_STORE_FP32 || (p->flags & PANNS_FLAG_LEARNED))
-            return fail(PANNS_EINVAL, "search: warps_per_query > 1 is for NSG_SEQ, TOP_M and PSS_V5 at T = 1 "
-                                      "with float32 storage, without PANNS_FLAG_LEARNED");
+        if (!ok || (p->flags & PANNS_FLAG_LEARNED))
+            return fail(PANNS_EINVAL, "search: warps_per_query > 1 is for NSG_SEQ, TOP_M and PSS_V5 at T = 1, "
+                                      "without PANNS_FLAG_LEARNED");
         if (h->max_deg > (uint32_t) kBuf)
             return fail(PANNS_EINVAL, "search: warps_per_query > 1 needs a graph degree <= " + std::to_string(kBuf));
     }
@@ -772,7 +772,7 @@ static int launch_search(panns_index *h, const panns_search_params *p, float *d_
     const uint32_t kind = p->distance == PANNS_DIST_L2 ? KIND_L2 : KIND_IP;
     const bool pss = p->mode == PANNS_MODE_PSS_V5 && p->T > 1;
     const uint32_t wpq = p->warps_per_query > 1 ? p->warps_per_query : 1u;
-    const void *kern = wpq > 1 ? search_block_kernel_ptr(kind, CL, wpq)
+    const void *kern = wpq > 1 ? search_block_kernel_ptr(kind, CL, wpq, p->storage)
                                : pss ? pss_kernel_ptr(kind, CL) : search_kernel_ptr(kind, order, CL, p->storage);
     if (!kern) return fail(PANNS_EINVAL, "search: unsupported dimension");
     const uint32_t M = p->mode == PANNS_MODE_TOP_M ? p->M : 1u;

@@ -166,6 +166,8 @@ def test_several_warps_per_query_small_batches_and_per_query_L(setup):
         ix.search(K=50, L=200, warps_per_query=3)
     with pytest.raises(N.PannsError):
         ix.search(K=50, L=200, mode=N.MODE_EFANNA, warps_per_query=2)
+    with pytest.raises(N.PannsError):
+        ix.search(K=50, L=200, mode=N.MODE_TOP_M, M=4, warps_per_query=2, flags=N.FLAG_LEARNED)
 
 
 @pytest.mark.parametrize("d", [8, 24, 128, 256])
@@ -194,3 +196,25 @@ def test_long_queue_default_block_shape(setup):
     got, _ = ix.search(q[:8], K=100, L=8192, mode=N.MODE_TOP_M, M=8)
     ref, _ = O.search_top_m(base, O.Graph.from_nsg(g), q[:8], 100, 8192, 8)
     assert np.array_equal(got, ref)
+
+
+@pytest.mark.parametrize("storage", [1, 2])
+def test_several_warps_per_query_reduced_storage(storage):
+    """BF16 / FP8 copies with 2 and 4 warps per query: same ids and counts as
+    one warp per query on the same copy (same distances, same re-rank)."""
+    from parallel_anns_b200 import datasets as ds
+    from parallel_anns_b200 import native as N
+    from parallel_anns_b200.searching import Index
+    base = ds.gaussian_mixture(20000, 96, seed=411, means_seed=411)
+    q = ds.gaussian_mixture(200, 96, seed=412, means_seed=411)
+    g = ds.build_nsg_graph(base, R=50, knn_k=64, device="cpu")
+    with Index(0) as ix:
+        ix.set_base(base, storage=storage)
+        ix.set_graph(g)
+        ix.set_queries(q)
+        for L, M, K in ((200, 8, 100), (257, 4, 10)):
+            ref, st = ix.search(K=K, L=L, mode=N.MODE_TOP_M, M=M, storage=storage)
+            for wq in (2, 4):
+                got, st2 = ix.search(K=K, L=L, mode=N.MODE_TOP_M, M=M, storage=storage, warps_per_query=wq)
+                assert np.array_equal(got, ref), (storage, L, wq)
+                assert st2["n_dist"] == st["n_dist"]
