@@ -235,7 +235,7 @@ def bench_ours(args):
     elif rank == 0:
         t0 = time.time()
         plain = AT.tune(handles[N.STORE_FP32], tune_q, tune_gt, K=K, target=RECALL_TARGET,
-                        storages=(N.STORE_FP32,), Ms=Ms, wpbs=(2, 4), wpqs=(1, 2, 4))
+                        storages=(N.STORE_FP32,), Ms=Ms, wpbs=(2, 4), wpqs=(1, 2, 4, 8))
         cands = [plain]
         for store in stores:
             if store == N.STORE_FP32 and model is None:
@@ -338,12 +338,12 @@ def bench_ours(args):
         # the head's own configuration, then the head's storage, L and M
         # without the learned prologue, with 1, 2 and 4 warps per query
         options = [(head.warps_per_query, ixh, dict(kw, flags=kw["flags"] | N.FLAG_CUDA_GRAPH))]
-        for wq in (1, 2, 4):
+        for wq in (1, 2, 4, 8):
             if wq == head.warps_per_query and head.learned is None:
                 continue  # the head itself
             options.append((wq, ixh, dict(kw, flags=N.FLAG_CUDA_GRAPH, warps_per_query=wq)))
         if head.storage != N.STORE_FP32:  # and the float32 rows with several warps
-            for wq in (2, 4):
+            for wq in (2, 4, 8):
                 options.append((wq, handles[N.STORE_FP32],
                                 dict(kw, storage=N.STORE_FP32, flags=N.FLAG_CUDA_GRAPH, warps_per_query=wq)))
         for wq, ixb, kwb in options:

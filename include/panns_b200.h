@@ -89,7 +89,7 @@ typedef struct {
                                 array to L1, which caches gathered rows. 0 = as many as fit,
                                 but no more than fit in 196 KB of shared memory */
     uint32_t warps_per_query; /* 0 or 1: one warp per query (warps_per_block queries per block);
-                                 2 or 4: that many warps share each query's steps (one query per
+                                 2, 4 or 8: that many warps share each query's steps (one query per
                                  block; NSG_SEQ, TOP_M, PSS_V5 at T = 1, any storage, no learned
                                  prologue), for small batches and long queues; same ids and counts */
 } panns_search_params;

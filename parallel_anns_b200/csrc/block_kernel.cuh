@@ -26,7 +26,7 @@
 
 namespace panns {
 
-constexpr int kBlockCtl = 16;  // control words in shared memory (BC_SEG + W <= 16)
+constexpr int kBlockCtl = 24;  // control words in shared memory (BC_SEG + W <= 24)
 
 // Shared memory of one block of W warps with a queue of queue_cap entries.
 __host__ __device__ inline uint32_t block_smem_bytes(uint32_t queue_cap, uint32_t W) {
@@ -37,7 +37,7 @@ __host__ __device__ inline uint32_t block_smem_bytes(uint32_t queue_cap, uint32_
            + kBlockCtl * 4u;                                          // control words
 }
 
-enum { BC_Q = 0, BC_SZ, BC_CNT, BC_LASTK, BC_K, BC_NK, BC_DIRTY, BC_DIST, BC_EDGES, BC_SEG };  // BC_SEG + w, w < W <= 4
+enum { BC_Q = 0, BC_SZ, BC_CNT, BC_LASTK, BC_K, BC_NK, BC_DIRTY, BC_DIST, BC_EDGES, BC_SEG };  // BC_SEG + w, w < W <= 8
 
 // Number of elements of the sorted list (d, k)[0..n) that precede (dv, kv).
 __device__ __forceinline__ uint32_t list_rank(const float *d, const uint32_t *k, uint32_t n, float dv, uint32_t kv) {

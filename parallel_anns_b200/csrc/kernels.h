@@ -28,7 +28,7 @@ inline const void *search_kernel_ptr(uint32_t kind, uint32_t order, int CL, uint
     return kind == 0 ? search_kernel_ptr_fp32_ip(kind, order, CL) : search_kernel_ptr_fp32_l2(kind, order, CL);
 }
 // search_block_kernel<KIND, CL, W, STORE> (block_kernel.cuh), W warps per
-// query; nullptr if not built (W other than 2 and 4).
+// query; nullptr if not built (W other than 2, 4 and 8).
 const void *search_block_kernel_ptr_fp32(uint32_t kind, int CL, uint32_t W);
 const void *search_block_kernel_ptr_bf16(uint32_t kind, int CL, uint32_t W);
 const void *search_block_kernel_ptr_fp8(uint32_t kind, int CL, uint32_t W);

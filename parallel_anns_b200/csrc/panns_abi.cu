@@ -645,8 +645,8 @@ int check_params(panns_index *h, const panns_search_params *p) {
         return fail(PANNS_EINVAL, "search: L_query is not supported by PSS_V5 with T > 1");
     if (p->storage > PANNS_STORE_FP8) return fail(PANNS_EINVAL, "search: unknown storage");
     if (p->warps_per_query > 1) {
-        if (p->warps_per_query != 2 && p->warps_per_query != 4)
-            return fail(PANNS_EINVAL, "search: warps_per_query must be 0, 1, 2 or 4");
+        if (p->warps_per_query != 2 && p->warps_per_query != 4 && p->warps_per_query != 8)
+            return fail(PANNS_EINVAL, "search: warps_per_query must be 0, 1, 2, 4 or 8");
         const bool ok = p->mode == PANNS_MODE_NSG_SEQ || p->mode == PANNS_MODE_TOP_M ||
                         (p->mode == PANNS_MODE_PSS_V5 && p->T == 1);
         if (!ok || (p->flags & PANNS_FLAG_LEARNED))

@@ -1,5 +1,5 @@
 // Several-warps-per-query search kernels (block_kernel.cuh): float32 rows, PANNS
-// order, both distance kinds, W in {2, 4}.
+// order, both distance kinds, W in {2, 4, 8}.
 #include "block_kernel.cuh"
 #include "kernels.h"
 
@@ -21,6 +21,7 @@ static const void *pick_block_cl(int CL) {
 const void *search_block_kernel_ptr_fp32(uint32_t kind, int CL, uint32_t W) {
     if (W == 2) return kind == KIND_IP ? pick_block_cl<KIND_IP, 2>(CL) : pick_block_cl<KIND_L2, 2>(CL);
     if (W == 4) return kind == KIND_IP ? pick_block_cl<KIND_IP, 4>(CL) : pick_block_cl<KIND_L2, 4>(CL);
+    if (W == 8) return kind == KIND_IP ? pick_block_cl<KIND_IP, 8>(CL) : pick_block_cl<KIND_L2, 8>(CL);
     return nullptr;
 }
 

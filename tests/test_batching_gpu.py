@@ -129,7 +129,7 @@ def test_autotuner_meets_target_on_tuning_queries(setup):
     assert c.kernel_ms == min(r["kernel_ms"] for r in rows)
 
 
-@pytest.mark.parametrize("wpq", [2, 4])
+@pytest.mark.parametrize("wpq", [2, 4, 8])
 @pytest.mark.parametrize("mode,M,L,dist", [(0, 1, 100, 0), (1, 4, 200, 0), (1, 8, 300, 1), (1, 64, 160, 0),
                                           (2, 1, 257, 1)])
 def test_several_warps_per_query_equal_one(setup, wpq, mode, M, L, dist):
@@ -214,7 +214,7 @@ def test_several_warps_per_query_reduced_storage(storage):
         ix.set_queries(q)
         for L, M, K in ((200, 8, 100), (257, 4, 10)):
             ref, st = ix.search(K=K, L=L, mode=N.MODE_TOP_M, M=M, storage=storage)
-            for wq in (2, 4):
+            for wq in (2, 4, 8):
                 got, st2 = ix.search(K=K, L=L, mode=N.MODE_TOP_M, M=M, storage=storage, warps_per_query=wq)
                 assert np.array_equal(got, ref), (storage, L, wq)
                 assert st2["n_dist"] == st["n_dist"]
