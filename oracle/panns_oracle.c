@@ -730,7 +730,7 @@ int po_ground_truth_fp64(const float *data, uint32_t n, uint32_t d,
 }
 
 /* ---- graph construction (restates parallel_anns_b200/csrc/graph_build.cu) ----
- * No PANNS counterpart: the graphs are built as BASELINE's configs describe
+ * No PANNS counterpart: the graphs the benchmark workloads describe
  * (exact k-NN, MRNG prune, medoid, reachability repair); the pruning rule is
  * efanna2e's sync_prune (include/efanna2e/index_nsg.cpp:233-283) on exact k-NN
  * lists, the repair plays the part of its tree_grow (:638-718). */
