@@ -502,7 +502,7 @@ def bench_reference(args):
     exe = os.path.join(ROOT, "oracle", "_ref", "ref_pss")
     if not os.path.exists(exe):
         print(json.dumps({"impl": "reference", "unavailable":
-                          "reference checker binaries were not built (oracle/_ref/ref_pss missing)"}))
+                          "reference binaries were not built (oracle/_ref/ref_pss missing)"}))
         return
     spec = workloads.SPECS[args.workload](n=args.n, nq=args.nq)
     dev = f"cuda:{local}" if torch.cuda.is_available() else "cpu"

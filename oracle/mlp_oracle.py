@@ -1,5 +1,5 @@
 """CPU oracle of the entry / L-budget network of panns_b200 — TEST
-INFRASTRUCTURE ONLY (imported by tests/ as the checker, never by the product).
+INFRASTRUCTURE ONLY (imported by tests/ to check the GPU results, never by the product).
 
 Restates, in float64 numpy, the network, loss and gradient that the GPU
 kernels of parallel_anns_b200/csrc/learned.cu compute (the parameter layout

@@ -1,8 +1,8 @@
 """ctypes wrapper of the CPU oracle (oracle/_ref/panns_oracle.so) and of the
-reference checker binaries (oracle/_ref/ref_*) — TEST INFRASTRUCTURE ONLY.
+reference binaries (oracle/_ref/ref_*) — TEST INFRASTRUCTURE ONLY.
 
 Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg import
-this module, and only as the checker. The product never does.
+this module, and only to check results. The product never does.
 """
 from __future__ import annotations
 
@@ -24,7 +24,7 @@ _lib = None
 
 
 def build(ref_root: str | None = None) -> None:
-    """Build the C oracle, and the reference checker binaries when the
+    """Build the C oracle, and the reference binaries when the
     reference sources are present."""
     targets = ["oracle"]
     env = dict(os.environ)
@@ -261,7 +261,7 @@ def recall_at(result_ids: np.ndarray, true_ids: np.ndarray, L: int, at: int = 10
     return hits / float(at * result_ids.shape[0])
 
 
-# --- reference checker binaries -------------------------------------------
+# --- reference binaries -------------------------------------------
 
 def ref_binary(name: str) -> str:
     return os.path.join(REF_DIR, name)
@@ -272,7 +272,7 @@ def have_ref() -> bool:
 
 
 def run_ref(name: str, out_path: str, env=None, **kw):
-    """Run a reference checker binary; returns (ids [nq x K], stats dict)."""
+    """Run a reference binary; returns (ids [nq x K], stats dict)."""
     args = [ref_binary(name)] + [f"{k}={v}" for k, v in kw.items()] + [f"out={out_path}"]
     r = subprocess.run(args, check=True, capture_output=True, text=True, env=env)
     stats = json.loads(r.stdout.strip().splitlines()[-1]) if r.stdout.strip() else {}

@@ -1,7 +1,7 @@
 /* CPU oracle for the PANNS search path — TEST INFRASTRUCTURE ONLY.
  *
  * A plain-C restatement of the reference's query-time search, used by tests/,
- * by __graft_entry__.smoke() and by bench.py's cpu_baseline leg as the checker.
+ * by __graft_entry__.smoke() and by bench.py's cpu_baseline leg, to check results.
  * The product never links, loads or calls it.
  *
  * Parity is pinned against the reference itself: the binaries built by

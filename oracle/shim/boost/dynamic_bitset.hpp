@@ -1,5 +1,5 @@
 // Minimal stand-in for boost::dynamic_bitset<>, used only to compile the
-// reference search sources into the checker binaries under oracle/_ref.
+// reference search sources into the reference binaries under oracle/_ref.
 // Boost is not installed in this image. The reference uses: a sized
 // constructor with an optional initial value (brace-initialised as
 // `flags{n, 0}`), operator[] for read and write, reset(), resize(), size().

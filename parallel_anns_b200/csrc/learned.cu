@@ -508,7 +508,7 @@ int kmeans_run(const float *rows, uint32_t n, uint32_t d, uint32_t k, uint32_t i
         // Last round: representatives of the final cells; otherwise new centroids.
         cell_kernel<<<k, 256, 0, s>>>(rows, d, dmem.p, doff.p, cent, it == iters ? rep : nullptr);
         LCU(cudaGetLastError());
-        LCU(cudaStreamSynchronize(s));  // the host vectors are rewritten next round
+        LCU(cudaStreamSynchronize(s));  // the host vectors are rewritten next iteration
     }
     // Empty cells: give each a row that no other cell uses.
     std::vector<uint32_t> h_rep(k);

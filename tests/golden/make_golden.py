@@ -1,6 +1,6 @@
 """Generate the golden fixtures of the search path from the reference itself.
 
-Run in a container that has the reference sources (its checker binaries are
+Run in a container that has the reference sources (its reference binaries are
 built by oracle/Makefile into oracle/_ref/):
 
     python tests/golden/make_golden.py

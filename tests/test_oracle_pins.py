@@ -2,7 +2,7 @@
 the reference's distances and norms and, id for id, the result lists and
 distance counts the reference produced for the committed golden fixtures
 (tests/golden/, generated by tests/golden/make_golden.py from the reference
-sources). Where the reference checker binaries are present (oracle/_ref), they
+sources). Where the reference binaries are present (oracle/_ref), they
 are re-run and must reproduce the fixtures too."""
 import ctypes
 import os
@@ -68,7 +68,7 @@ def test_oracle_reproduces_reference_ids(case, golden_manifest):
         assert nd == spec["n_dist"], f"{case}/{form}: n_dist {nd} != {spec['n_dist']}"
 
 
-@pytest.mark.skipif(not O.have_ref(), reason="reference checker binaries not built here")
+@pytest.mark.skipif(not O.have_ref(), reason="reference binaries not built here")
 @pytest.mark.parametrize("case", ["mix3k_d96", "mix1k_d24"])
 def test_reference_binaries_reproduce_fixtures(case, golden_manifest):
     d = os.path.join(GOLDEN, case)
@@ -112,7 +112,7 @@ def test_pss_many_workers_recall_close_to_single(golden_manifest):
         assert abs(O.recall_at(rt, tid, 200) - base_rec) < 0.01
 
 
-@pytest.mark.skipif(not O.have_ref(), reason="reference checker binaries not built here")
+@pytest.mark.skipif(not O.have_ref(), reason="reference binaries not built here")
 @pytest.mark.parametrize("T,X", [(2, 1), (4, 2), (8, 4)])
 def test_pss_workers_against_reference(T, X):
     """PSS_v5 at T > 1 is not deterministic in the reference (its workers race
