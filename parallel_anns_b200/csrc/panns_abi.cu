@@ -771,7 +771,17 @@ static int launch_search(panns_index *h, const panns_search_params *p, float *d_
     const uint32_t order = p->mode == PANNS_MODE_EFANNA ? ORDER_EFANNA : ORDER_PANNS;
     const uint32_t kind = p->distance == PANNS_DIST_L2 ? KIND_L2 : KIND_IP;
     const bool pss = p->mode == PANNS_MODE_PSS_V5 && p->T > 1;
-    const uint32_t wpq = p->warps_per_query > 1 ? p->warps_per_query : 1u;
+    uint32_t wpq = p->warps_per_query > 1 ? p->warps_per_query : 1u;
+    if (p->warps_per_query == 0 && p->warps_per_block == 0 && p->blocks_per_sm == 0 &&
+        (p->mode == PANNS_MODE_NSG_SEQ || p->mode == PANNS_MODE_TOP_M || (p->mode == PANNS_MODE_PSS_V5 && p->T == 1)) &&
+        !(p->flags & PANNS_FLAG_LEARNED) && h->max_deg <= (uint32_t) kBuf) {
+        // Automatic block shape (same ids either way), from the 1M x 96 and
+        // 1M x 128 measurements: 8 warps per query up to one query per SM and
+        // for queues of 2048 and more, 2 up to ten queries per SM, else one.
+        const uint32_t sms = (uint32_t) h->num_sms;
+        if (p->L >= 2048 || nq <= sms) wpq = 8;
+        else if (nq <= 10 * sms) wpq = 2;
+    }
     const void *kern = wpq > 1 ? search_block_kernel_ptr(kind, CL, wpq, p->storage)
                                : pss ? pss_kernel_ptr(kind, CL) : search_kernel_ptr(kind, order, CL, p->storage);
     if (!kern) return fail(PANNS_EINVAL, "search: unsupported dimension");

@@ -136,7 +136,7 @@ def test_several_warps_per_query_equal_one(setup, wpq, mode, M, L, dist):
     """warps_per_query 2 / 4 return the one-warp kernel's ids and counts (and the oracle's)."""
     ix, N, base, q, g = setup
     K = min(100, L)
-    ref, st = ix.search(K=K, L=L, mode=mode, M=M, distance=dist)
+    ref, st = ix.search(K=K, L=L, mode=mode, M=M, distance=dist, warps_per_query=1)
     got, st2 = ix.search(K=K, L=L, mode=mode, M=M, distance=dist, warps_per_query=wpq)
     assert np.array_equal(got, ref)
     assert st2["n_dist"] == st["n_dist"] and st2["n_iter"] == st["n_iter"]
@@ -151,7 +151,7 @@ def test_several_warps_per_query_small_batches_and_per_query_L(setup):
     import torch
     ix, N, base, q, g = setup
     Lq = np.random.default_rng(3).choice([64, 100, 200], size=q.shape[0]).astype(np.uint32)
-    ref, _ = ix.search(K=50, L=200, mode=1, M=8, L_query=Lq)
+    ref, _ = ix.search(K=50, L=200, mode=1, M=8, L_query=Lq, warps_per_query=1)
     got, _ = ix.search(K=50, L=200, mode=1, M=8, L_query=Lq, warps_per_query=4)
     assert np.array_equal(got, ref)
     qd = torch.from_numpy(q[:5]).cuda()
@@ -182,7 +182,7 @@ def test_several_warps_per_query_dimensions(N_lib, d):
         ix.set_graph(g)
         ix.set_queries(q)
         for dist in (0, 1):
-            ref, st = ix.search(K=50, L=120, mode=1, M=4, distance=dist)
+            ref, st = ix.search(K=50, L=120, mode=1, M=4, distance=dist, warps_per_query=1)
             got, st2 = ix.search(K=50, L=120, mode=1, M=4, distance=dist, warps_per_query=2)
             assert np.array_equal(got, ref) and st["n_dist"] == st2["n_dist"]
 
@@ -213,7 +213,7 @@ def test_several_warps_per_query_reduced_storage(storage):
         ix.set_graph(g)
         ix.set_queries(q)
         for L, M, K in ((200, 8, 100), (257, 4, 10)):
-            ref, st = ix.search(K=K, L=L, mode=N.MODE_TOP_M, M=M, storage=storage)
+            ref, st = ix.search(K=K, L=L, mode=N.MODE_TOP_M, M=M, storage=storage, warps_per_query=1)
             for wq in (2, 4, 8):
                 got, st2 = ix.search(K=K, L=L, mode=N.MODE_TOP_M, M=M, storage=storage, warps_per_query=wq)
                 assert np.array_equal(got, ref), (storage, L, wq)

@@ -31,27 +31,30 @@ def gpu_index(base, g, queries=None):
     return ix
 
 
-def gpu_form(ix, N, spec):
-    """Run the GPU counterpart of a golden form."""
+def gpu_form(ix, N, spec, wpq=0):
+    """Run the GPU counterpart of a golden form (wpq: warps per query; 0 =
+    the library's automatic choice, which for these small batches is a block
+    of 8 warps per query where the form allows it)."""
     a, b = spec["args"], spec["binary"]
     K, L = a["K"], a["L"]
     if b in ("ref_pss", "ref_pss_lg"):
         dist = N.DIST_NORM_IP if b == "ref_pss" else N.DIST_L2
-        return ix.search(K=K, L=L, mode=N.MODE_PSS_V5, distance=dist, T=a["T"], X=a["X"])
+        return ix.search(K=K, L=L, mode=N.MODE_PSS_V5, distance=dist, T=a["T"], X=a["X"], warps_per_query=wpq)
     if b == "ref_topm":
         if a["mode"] == "simple":
-            return ix.search(K=K, L=L, mode=N.MODE_NSG_SEQ, distance=N.DIST_NORM_IP)
-        return ix.search(K=K, L=L, mode=N.MODE_TOP_M, distance=N.DIST_NORM_IP, M=a["M"])
+            return ix.search(K=K, L=L, mode=N.MODE_NSG_SEQ, distance=N.DIST_NORM_IP, warps_per_query=wpq)
+        return ix.search(K=K, L=L, mode=N.MODE_TOP_M, distance=N.DIST_NORM_IP, M=a["M"], warps_per_query=wpq)
     dist = N.DIST_L2 if a["mode"] == "search" else N.DIST_NORM_IP
     return ix.search(K=K, L=L, mode=N.MODE_EFANNA, distance=dist)
 
 
+@pytest.mark.parametrize("wpq", [1, 0])
 @pytest.mark.parametrize("case", CASES)
-def test_gpu_matches_reference_golden(case, golden_manifest, N):
+def test_gpu_matches_reference_golden(case, golden_manifest, N, wpq):
     base, q, g, _ = load_case(case)
     ix = gpu_index(base, g, q)
     for form, spec in golden_manifest[case]["forms"].items():
-        ids, st = gpu_form(ix, N, spec)
+        ids, st = gpu_form(ix, N, spec, wpq)
         ref = golden_ids(case, form, spec["args"]["K"])
         bad = np.nonzero((ids != ref).any(1))[0]
         assert bad.size == 0, f"{case}/{form}: rows {bad[:8].tolist()} differ"
@@ -68,15 +71,16 @@ def mix20k():
     return base, q, g
 
 
+@pytest.mark.parametrize("wpq", [1, 0])
 @pytest.mark.parametrize("L,M", [(64, 1), (100, 1), (333, 1), (100, 2), (200, 8), (128, 32), (96, 64)])
-def test_gpu_top_m_matches_oracle(mix20k, N, L, M):
+def test_gpu_top_m_matches_oracle(mix20k, N, L, M, wpq):
     base, q, g = mix20k
     G = O.Graph.from_nsg(g)
     ix = gpu_index(base, g, q)
     K = min(100, L)
     mode = N.MODE_NSG_SEQ if M == 1 else N.MODE_TOP_M
     for dist, kind in ((N.DIST_NORM_IP, O.DIST_IP_NORM), (N.DIST_L2, O.DIST_L2)):
-        ids, st = ix.search(K=K, L=L, mode=mode, distance=dist, M=M)
+        ids, st = ix.search(K=K, L=L, mode=mode, distance=dist, M=M, warps_per_query=wpq)
         ref, nd = O.search_top_m(base, G, q, K, L, M, kind=kind)
         assert np.array_equal(ids, ref), f"L={L} M={M} dist={dist}: {(ids != ref).any(1).sum()} rows"
         assert st["n_dist"] == nd
@@ -128,7 +132,8 @@ def test_gpu_dimensions(N, d):
     ix.close()
 
 
-def test_gpu_edge_graphs(N):
+@pytest.mark.parametrize("wpq", [1, 0])
+def test_gpu_edge_graphs(N, wpq):
     """Zero-degree vertices, a hub with more neighbours than one head row holds,
     L = N (every vertex in the queue), K = 1, a single query."""
     from parallel_anns_b200.formats import NSGGraph
@@ -145,7 +150,7 @@ def test_gpu_edge_graphs(N):
     for L, K, M in ((10, 10, 1), (40, 1, 1), (n, 100, 1), (n, 5, 7), (64, 64, 64)):
         mode = N.MODE_NSG_SEQ if M == 1 else N.MODE_TOP_M
         for dist, kind in ((N.DIST_NORM_IP, O.DIST_IP_NORM), (N.DIST_L2, O.DIST_L2)):
-            ids, st = ix.search(K=K, L=L, mode=mode, distance=dist, M=M)
+            ids, st = ix.search(K=K, L=L, mode=mode, distance=dist, M=M, warps_per_query=wpq)
             ref, nd = O.search_top_m(base, G, q, K, L, M, kind=kind)
             assert np.array_equal(ids, ref), (L, K, M, dist)
             assert st["n_dist"] == nd
