@@ -70,6 +70,7 @@ constexpr int kBuf = PANNS_KBUF;  // fresh-candidate buffer per warp
 static_assert(kBuf >= 64 && (kBuf & (kBuf - 1)) == 0, "kBuf must be a power of two >= 64");
 constexpr int kCandGroup = 8;    // candidates whose head rows are staged at once
 constexpr int kGroupChunks = (kCandGroup * kHeadNbrs + 31) / 32;
+constexpr int kOvfChunks = 2;    // overflow neighbours per batch of loads: kOvfChunks * 32
 constexpr int kMaxM = 64;
 
 enum { ORDER_PANNS = 0, ORDER_EFANNA = 1 };
@@ -805,6 +806,9 @@ __device__ void search_one(const SearchArgs &a, const WarpMem &m, uint32_t q, ui
             const uint32_t gc = min((uint32_t) kCandGroup, cnt - c0);
             // Stage the head rows: one warp-wide 128-byte load per candidate,
             // all issued before the first store.
+            // Lane j < gc also fetches candidate j's overflow offset (used if
+            // its row is longer than the head row), in flight with the rows.
+            const uint64_t my_off = (uint32_t) lane < gc ? __ldg(a.ovf_off + m.cand[c0 + lane]) : 0ull;
             {
                 uint32_t hv[kCandGroup];
 #pragma unroll
@@ -865,23 +869,51 @@ __device__ void search_one(const SearchArgs &a, const WarpMem &m, uint32_t q, ui
                 note_dirty(dirty, a.dirty_cap, dcount, valid && olds[ch] == 0, id >> 5);
                 append_fresh<KIND, ORDER, CL, STORE>(a, m, nb, &sz, L, nk, n_dist, fresh, id, D, lane);
             }
-            // Rows longer than the head row: the rest from the overflow list.
+            // Rows longer than the head row: the rest from the overflow lists
+            // of all the group's long candidates, flattened in (candidate,
+            // slot) order; per batch of kOvfChunks * 32 every load is issued
+            // before any test-and-set, and every test-and-set before any
+            // result is used.
             if (any_long) {
-                for (uint32_t j = 0; j < gc; ++j) {
-                    const uint32_t dj = m.hrow[j * kHeadWords];
-                    if (dj <= (uint32_t) kHeadNbrs) continue;
-                    const uint64_t off = __ldg(a.ovf_off + m.cand[c0 + j]);
-                    for (uint32_t s0 = kHeadNbrs; s0 < dj; s0 += 32) {
-                        const uint32_t s = s0 + lane;
-                        bool valid = s < dj;
-                        const uint32_t id = valid ? __ldg(a.ovf + off + (s - kHeadNbrs)) : 0u;
-                        if (valid && id >= a.n) {
+                const uint32_t ocount = deg > (uint32_t) kHeadNbrs ? deg - kHeadNbrs : 0u;  // 0 for lanes >= gc
+                uint32_t oincl = ocount;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t t = __shfl_up_sync(kFull, oincl, o);
+                    if (lane >= o) oincl += t;
+                }
+                const uint32_t ototal = __shfl_sync(kFull, oincl, 31);
+                const uint32_t oexcl = oincl - ocount;
+                for (uint32_t f0 = 0; f0 < ototal; f0 += 32 * kOvfChunks) {
+                    uint32_t oid[kOvfChunks], oold[kOvfChunks];
+#pragma unroll
+                    for (int ch = 0; ch < kOvfChunks; ++ch) {
+                        const uint32_t f = f0 + ch * 32 + lane;
+                        // owner: the last candidate whose flattened range starts at or before f
+                        uint32_t j = 0;
+                        for (uint32_t t = 1; t < gc; ++t)
+                            if (__shfl_sync(kFull, oexcl, t) <= f) j = t;
+                        const uint32_t pj = __shfl_sync(kFull, oexcl, j);
+                        const uint64_t offj = __shfl_sync(kFull, my_off, j);
+                        oid[ch] = f < ototal ? __ldg(a.ovf + offj + (f - pj)) : kFull;
+                    }
+#pragma unroll
+                    for (int ch = 0; ch < kOvfChunks; ++ch) {
+                        bool valid = oid[ch] != kFull;
+                        if (valid && oid[ch] >= a.n) {
                             atomicOr(a.error, ERR_BAD_ID);
                             valid = false;
+                            oid[ch] = kFull;
                         }
-                        const uint32_t old = visit_issue(vis, id, valid);
-                        const bool fresh = valid && !(old & (1u << (id & 31)));
-                        note_dirty(dirty, a.dirty_cap, dcount, valid && old == 0, id >> 5);
+                        oold[ch] = visit_issue(vis, oid[ch], valid);
+                    }
+#pragma unroll
+                    for (int ch = 0; ch < kOvfChunks; ++ch) {
+                        if (f0 + ch * 32 >= ototal) break;
+                        const uint32_t id = oid[ch];
+                        const bool valid = id != kFull;
+                        const bool fresh = valid && !(oold[ch] & (1u << (id & 31)));
+                        note_dirty(dirty, a.dirty_cap, dcount, valid && oold[ch] == 0, id >> 5);
                         append_fresh<KIND, ORDER, CL, STORE>(a, m, nb, &sz, L, nk, n_dist, fresh, id, D, lane);
                     }
                 }
