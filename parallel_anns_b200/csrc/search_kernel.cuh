@@ -331,20 +331,21 @@ __device__ void warp_sort(float *bd, uint32_t *bi, uint32_t *bk, uint32_t cnt,
         bk[i] = kFull;
     }
     __syncwarp();
+    // One compare-exchange pair per lane and pass: pair p has its lower index
+    // i = p with a zero bit inserted at bit j, its upper one i | j.
     for (uint32_t k = 2; k <= n; k <<= 1) {
         for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-            for (uint32_t i = lane; i < n; i += 32) {
-                const uint32_t ixj = i ^ j;
-                if (ixj > i) {
-                    const float ad = bd[i], xd = bd[ixj];
-                    const uint32_t ak = bk[i], xk = bk[ixj];
-                    const bool up = (i & k) == 0;
-                    const bool sw = up ? plain_less(xd, xk, ad, ak) : plain_less(ad, ak, xd, xk);
-                    if (sw) {
-                        bd[i] = xd; bd[ixj] = ad;
-                        bk[i] = xk; bk[ixj] = ak;
-                        const uint32_t t = bi[i]; bi[i] = bi[ixj]; bi[ixj] = t;
-                    }
+            for (uint32_t p = lane; p < (n >> 1); p += 32) {
+                const uint32_t i = ((p & ~(j - 1)) << 1) | (p & (j - 1));
+                const uint32_t ixj = i | j;
+                const float ad = bd[i], xd = bd[ixj];
+                const uint32_t ak = bk[i], xk = bk[ixj];
+                const bool up = (i & k) == 0;
+                const bool sw = up ? plain_less(xd, xk, ad, ak) : plain_less(ad, ak, xd, xk);
+                if (sw) {
+                    bd[i] = xd; bd[ixj] = ad;
+                    bk[i] = xk; bk[ixj] = ak;
+                    const uint32_t t = bi[i]; bi[i] = bi[ixj]; bi[ixj] = t;
                 }
             }
             __syncwarp();
@@ -603,20 +604,19 @@ static __device__ void rank_sort(float *qd, uint32_t *qi, uint32_t sz, const uin
     __syncwarp();
     for (uint32_t k = 2; k <= n; k <<= 1) {
         for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-            for (uint32_t i = lane; i < n; i += 32) {
-                const uint32_t ixj = i ^ j;
-                if (ixj > i) {
-                    const float ad = qd[i], xd = qd[ixj];
-                    const uint32_t ai = qi[i], xi = qi[ixj];
-                    const uint32_t ak = ai == kFull ? kFull : (ai & kIdMask);
-                    const uint32_t xk = xi == kFull ? kFull : (xi & kIdMask);
-                    const bool up = (i & k) == 0;
-                    const bool sw = up ? key_less<ORDER_PANNS>(xd, xk, ad, ak, orig)
-                                       : key_less<ORDER_PANNS>(ad, ak, xd, xk, orig);
-                    if (sw) {
-                        qd[i] = xd; qd[ixj] = ad;
-                        qi[i] = xi; qi[ixj] = ai;
-                    }
+            for (uint32_t p = lane; p < (n >> 1); p += 32) {  // pairs, as in warp_sort
+                const uint32_t i = ((p & ~(j - 1)) << 1) | (p & (j - 1));
+                const uint32_t ixj = i | j;
+                const float ad = qd[i], xd = qd[ixj];
+                const uint32_t ai = qi[i], xi = qi[ixj];
+                const uint32_t ak = ai == kFull ? kFull : (ai & kIdMask);
+                const uint32_t xk = xi == kFull ? kFull : (xi & kIdMask);
+                const bool up = (i & k) == 0;
+                const bool sw = up ? key_less<ORDER_PANNS>(xd, xk, ad, ak, orig)
+                                   : key_less<ORDER_PANNS>(ad, ak, xd, xk, orig);
+                if (sw) {
+                    qd[i] = xd; qd[ixj] = ad;
+                    qi[i] = xi; qi[ixj] = ai;
                 }
             }
             __syncwarp();
