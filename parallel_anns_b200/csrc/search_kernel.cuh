@@ -833,7 +833,11 @@ __device__ void search_one(const SearchArgs &a, const WarpMem &m, uint32_t q, ui
                 if (lane >= o) incl += t;
             }
             const uint32_t total = __shfl_sync(kFull, incl, 31);
-            if (lane < (int) gc) m.pre[lane] = incl - hcount;
+            // Start of each candidate's neighbours in the flattened list, in
+            // registers of every lane (lanes >= gc hold total, past every f).
+            uint32_t pre_r[kCandGroup];
+#pragma unroll
+            for (int t = 0; t < kCandGroup; ++t) pre_r[t] = __shfl_sync(kFull, incl - hcount, t);
             uint32_t degsum = deg;
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) degsum += __shfl_xor_sync(kFull, degsum, o);
@@ -849,9 +853,14 @@ __device__ void search_one(const SearchArgs &a, const WarpMem &m, uint32_t q, ui
                 uint32_t id = 0;
                 bool valid = f < total;
                 if (valid) {
-                    uint32_t j = 0;
-                    while (j + 1 < gc && m.pre[j + 1] <= f) ++j;
-                    id = m.hrow[j * kHeadWords + 1 + (f - m.pre[j])];
+                    uint32_t j = 0, pj = 0;  // owner: the last candidate starting at or before f
+#pragma unroll
+                    for (int t = 1; t < kCandGroup; ++t)
+                        if (pre_r[t] <= f) {
+                            j = t;
+                            pj = pre_r[t];
+                        }
+                    id = m.hrow[j * kHeadWords + 1 + (f - pj)];
                     if (id >= a.n) {
                         atomicOr(a.error, ERR_BAD_ID);
                         valid = false;
