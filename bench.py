@@ -160,6 +160,79 @@ def cpu_model():
     return "unknown"
 
 
+def host_workload(spec, log):
+    """The workload's inputs built on the host CPU without the GPU library:
+    vectors from the same seeded generator, then the graph and the float64
+    ground truth by oracle/host_build.c (exact: the same graph as the GPU
+    construction and the same top-k as a float64 brute force). The
+    reference arm uses this, so its process never maps the library."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from parallel_anns_b200 import workloads
+    t0 = time.time()
+    base = workloads.vectors(spec, spec["n"], spec["base_seed"])
+    q = workloads.vectors(spec, spec["nq"], spec["query_seed"])
+    t1 = time.time()
+    g, _ = O.host_build_nsg(base, spec["knn_k"], spec["R"])
+    t2 = time.time()
+    gt_ids, gt_d = O.host_knn(base, q, spec["gt_k"])
+    t3 = time.time()
+    return workloads.store(spec, base, q, g, gt_ids, gt_d, HOST_BUILT,
+                           {"generate": t1 - t0, "graph": t2 - t1, "ground_truth": t3 - t2}, log=log)
+
+
+HOST_BUILT = "host CPU (oracle/host_build.c)"
+
+
+def check_host_inputs(W, spec, local, log):
+    """When the cached inputs were built on the host, rebuild the graph and the
+    ground truth on the GPU and compare them byte for byte."""
+    import numpy as np
+    from parallel_anns_b200 import workloads
+    from parallel_anns_b200.graph import build_nsg
+    built_by = W["meta"].get("built_by", "gpu")
+    out = {"built_by": built_by}
+    if built_by != HOST_BUILT:
+        return out
+    g, h = build_nsg(W["base"], R=spec["R"], knn_k=spec["knn_k"], device=local), W["graph"]
+    same_g = (g.entry == h.entry and g.width == h.width and np.array_equal(g.offsets, h.offsets)
+              and np.array_equal(g.nbrs, h.nbrs))
+    gt, _ = workloads.ground_truth(W["base"], h, W["queries"], spec["gt_k"], f"cuda:{local}")
+    same_gt = bool(np.array_equal(gt, W["gt"]))
+    out["gpu_rebuild_identical"] = bool(same_g and same_gt)
+    if not out["gpu_rebuild_identical"]:
+        log(f"inputs: GPU rebuild differs from the host-built files (graph {same_g}, ground truth {same_gt})")
+    return out
+
+
+def parity_sample(index, choice, paths, K, nq_sample, log):
+    """Ids of the exact FP32 search at the plain operating point against the
+    reference's own top-M search at one thread (oracle/_ref/ref_topm: the
+    sequential search for M = 1, para_search_with_top_m_pure otherwise) on the
+    first nq_sample evaluation queries: rows equal, distance counts equal."""
+    import numpy as np
+    from parallel_anns_b200 import native as N
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_topm")
+    if not os.path.exists(exe):
+        return {"unavailable": "oracle/_ref/ref_topm not built"}
+    mode = "simple" if choice.M == 1 else "topm_para"
+    with tempfile.TemporaryDirectory() as tmp:
+        out = os.path.join(tmp, "ids.bin")
+        r = subprocess.run([exe, f"data={paths['base']}", f"queries={paths['query']}", f"nsg={paths['graph']}",
+                            f"K={K}", f"L={choice.L}", f"M={choice.M}", f"mode={mode}", "T=1",
+                            f"nq={nq_sample}", f"out={out}"], check=True, capture_output=True, text=True,
+                           timeout=900)
+        ref = np.fromfile(out, dtype=np.uint32).reshape(-1, K)
+    st_ref = json.loads(r.stdout.strip().splitlines()[-1])
+    kw = dict(choice.search_kwargs(), storage=N.STORE_FP32, flags=0)
+    ids, st = index.search(K=K, q_begin=0, nq=nq_sample, distance=N.DIST_NORM_IP, **kw)
+    rows_equal = int((ids == ref).all(1).sum())
+    res = {"queries": nq_sample, "rows_equal": rows_equal, "n_dist_equal": int(st["n_dist"]) == int(st_ref["n_dist"]),
+           "n_dist": int(st["n_dist"]), "reference": f"ref_topm {mode} T=1 L={choice.L} M={choice.M}"}
+    log(f"parity sample: {res}")
+    return res
+
+
 # ---------------------------------------------------------------------------
 def bench_ours(args):
     import numpy as np
@@ -194,6 +267,7 @@ def bench_ours(args):
         W = workloads.load(spec)
         if not fixed:
             tune_q, tune_gt = workloads.tuning_set(spec, W)
+    inputs = check_host_inputs(W, spec, local, log) if rank == 0 else None
     q_all, gt_all = W["queries"], W["gt"]
     qs = np.ascontiguousarray(q_all[shard(rank, args.nq)])
     gts = gt_all[shard(rank, args.nq)]
@@ -404,53 +478,53 @@ def bench_ours(args):
     value = total_q / (kernel_ms_max / 1e3)
     e2e_value = total_q / e2e_s
 
-    cpu_base = None
+    cpu_base, parity = None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu_base = cpu_baseline(W["paths"], plain.L, nq, log)
+    if rank == 0 and not args.no_parity:
+        try:
+            parity = parity_sample(handles[N.STORE_FP32], plain, W["paths"], K, min(500, nq), log)
+        except Exception as e:  # reported, never fatal
+            parity = {"unavailable": str(e)[:200]}
 
     if world > 1:
         dist.barrier()
     if rank == 0:
+        details = {"autotune": choices["tables"], "batching": batching, "cpu_baseline": cpu_base,
+                   "learned": learned_info, "inputs": inputs}
+        log("details " + json.dumps(details))
+        # The JSON line stays short (the full tables go to stderr above).
         line = {
             "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
             "steps": steps, "warmup": args.warmup,
             "ms_per_step": round(kernel_ms_max / steps, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": names[store], "data": "synthetic",
             "config": {"workload": "batched search, " + workloads.describe(spec) + " (per GPU)",
-                       "n": args.n, "d": d, "queries_per_gpu": nq, "K": K, "L": L, "M": M,
-                       "warps_per_block": head.warps_per_block, "warps_per_query": head.warps_per_query,
-                       "blocks_per_sm": head.blocks_per_sm,
+                       "L": L, "M": M, "warps_per_block": head.warps_per_block,
+                       "warps_per_query": head.warps_per_query, "blocks_per_sm": head.blocks_per_sm,
                        "storage": names[store], "accumulate": "f32",
                        "rerank": "exact f32 of the final L" if store != N.STORE_FP32 else None,
-                       "learned": learned_info,
+                       "learned": None if learned_info is None else learned_info["options"],
                        "mode": "NSG_SEQ" if M == 1 else "TOP_M", "distance": "NORM_IP",
-                       "recall100": round(rec, 5), "recall_target": RECALL_TARGET,
-                       "mean_rel_distance_error_vs_fp64": dist_err,
-                       "avg_degree": round(W["meta"]["avg_degree"], 3), "width": W["meta"]["width"],
+                       "recall100": round(rec, 5), "rel_dist_err_vs_fp64": float(f"{dist_err:.3g}"),
                        "parallelism": f"replicas x{world}",
-                       "operating_point": ("fixed by --L/--M" if fixed else
-                                           "autotuned on 10k held-out tuning queries (another seed); "
-                                           "recall and speed measured on the 10k evaluation queries"),
-                       "l2": f"inputs larger than L2 ({args.n * d * 4 >> 20} MB base) and a 256 MB L2 flush "
-                             "before each step",
-                       "autotune": choices["tables"]},
+                       "operating_point": "fixed by --L/--M" if fixed else "autotuned on 10k held-out queries",
+                       "l2": "inputs > L2 and a 256 MB L2 flush before each step",
+                       "inputs": inputs},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
-                         "frac": round(achieved / peak, 4), "traffic": traffic,
-                         "peak_source": peak_kind,
-                         "algorithmic_bytes_per_launch": int(alg_bytes)},
+                         "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_kind},
             "e2e": {"value": round(e2e_value, 1), "unit": UNIT,
                     "h2d_bytes_per_step": nq * d * 4,
                     "d2h_bytes_per_step": nq * K * 4 + nq * 16 + 4},
             "gpu_launches": steps,
-            "plain_fp32": {"value": round(nq * world * steps / (p_ms_max / 1e3), 1), "unit": UNIT,
-                           "L": plain.L, "M": plain.M, "warps_per_block": plain.warps_per_block,
-                           "warps_per_query": plain.warps_per_query,
-                           "recall100": round(p_rec, 5), "ms_per_step": round(p_ms_max / steps, 4),
+            "plain_fp32": {"value": round(nq * world * steps / (p_ms_max / 1e3), 1),
+                           "L": plain.L, "M": plain.M, "warps_per_query": plain.warps_per_query,
+                           "recall100": round(p_rec, 5),
                            "roofline_frac": round(p_alg / (p_ms / steps / 1e3) / 1e9 / peak, 4)},
-            "batching": batching,
-            "counts_per_query": {k: round(v / steps / nq, 2) for k, v in tot.items()},
+            "parity": parity,
+            "batching_qps": {b: v["qps"] for b, v in batching.items()},
             "clocks": clocks,
-            "cpu_baseline": cpu_base,
+            "cpu_baseline": None if cpu_base is None else {k: v for k, v in cpu_base.items() if k != "modes"},
         }
         print(json.dumps(line), flush=True)
     for ixx in set(handles.values()):
@@ -498,15 +572,23 @@ def bench_reference(args):
     if rank != 0:
         return
     from parallel_anns_b200 import workloads
-    import torch
     exe = os.path.join(ROOT, "oracle", "_ref", "ref_pss")
     if not os.path.exists(exe):
         print(json.dumps({"impl": "reference", "unavailable":
                           "reference binaries were not built (oracle/_ref/ref_pss missing)"}))
         return
     spec = workloads.SPECS[args.workload](n=args.n, nq=args.nq)
-    dev = f"cuda:{local}" if torch.cuda.is_available() else "cpu"
-    W = workloads.build(spec, device=dev, log=log)
+    # Inputs: the cached files if present, else built on the host (no GPU
+    # library in this process).
+    if workloads.cached(spec):
+        W = workloads.load(spec)
+    elif spec.get("kind") == "uint8":
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "the integer-valued workload's inputs are built on the GPU only (no cluster "
+                          "structure for the host builder); run the GPU arm first"}))
+        return
+    else:
+        W = host_workload(spec, log)
     T = nproc()
     # The reference's own operating point: smallest swept L with recall@100 >= 0.95
     # on a sample, measured by the reference itself.
@@ -565,6 +647,7 @@ def main():
                     help="fix the storage (0 fp32, 1 bf16, 2 fp8; default: sweep)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="leave the learned entry network out")
+    ap.add_argument("--no-parity", action="store_true", help="skip the id check against the reference")
     ap.add_argument("--wpb", type=int, default=2, help="warps per block with a fixed --L and --M")
     ap.add_argument("--workload", default="mixture_1m_d96", choices=["mixture_1m_d96", "u8_1m_d128"],
                     help="mixture_1m_d96: the batched-FP32 config (default); u8_1m_d128: the "

@@ -197,9 +197,12 @@ int panns_search_device(panns_index *h, const panns_search_params *p, const floa
  * handle's stream). Modes NSG_SEQ, TOP_M and PSS_V5 with T = 1 (the PANNS init
  * list), L <= 1024. All scratch comes from one fixed 32 MiB array in the
  * library's device image: N, nq and the warp count must fit it, otherwise
- * PANNS_EINVAL says so. The index must already be laid out on the GPU (one
- * panns_search or panns_search_host call before). The first call on a device
- * looks up the array's address; make it before any stream capture. Calls
+ * PANNS_EINVAL says so. One warp per query with as many blocks per SM as
+ * fit: warps_per_query > 1 or blocks_per_sm != 0 give PANNS_EINVAL. The index
+ * must already be laid out on the GPU (one panns_search or panns_search_host
+ * call before). The first call on a device looks up the array's address. Do
+ * not call it while a stream is being captured: every call copies the init
+ * list from host memory, reads the error word back and synchronises. Calls
  * share the array: calls that overlap on the GPU race. Returns after the
  * search has finished. */
 int panns_search_static(panns_index *h, const panns_search_params *p, const float *d_queries,

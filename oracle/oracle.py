@@ -65,6 +65,8 @@ def lib():
         L.po_search_efanna.argtypes = [P, P, u32, u32, P, P, P, u32, P, u32, u32, ctypes.c_int,
                                        P, P, ctypes.c_int]
         L.po_ground_truth_fp64.argtypes = [P, u32, u32, P, u32, u32, P, P, ctypes.c_int]
+        L.po_host_knn.argtypes = [P, u32, u32, P, u32, u32, P, P, ctypes.c_int]
+        L.po_host_build_nsg.argtypes = [P, u32, u32, u32, u32, P, P, P, P, ctypes.c_uint64, P, ctypes.c_int]
         _lib = L
     return _lib
 
@@ -298,5 +300,45 @@ def build_nsg(base, k, R, threads=0):
                             _threads(threads))
     if rc:
         raise ValueError(f"po_build_nsg failed ({rc})")
+    g = NSGGraph(int(width[0]), int(entry[0]), off.astype(np.int64), nbrs[:int(off[-1])].copy())
+    return g, knn
+
+
+def host_knn(base, queries, k, threads=0):
+    """Exact top-k by (float64 FMA-chain distance, id) with cluster lower
+    bounds (oracle/host_build.c); queries=None: the k-NN of every base row,
+    itself excluded. Returns (ids u32 [nq x k], float64 distances)."""
+    x = np.ascontiguousarray(base, dtype=np.float32)
+    n, d = x.shape
+    if queries is None:
+        qp, nq = None, n
+    else:
+        queries = np.ascontiguousarray(queries, dtype=np.float32)
+        qp, nq = _p(queries), queries.shape[0]
+    ids = np.empty((nq, k), dtype=np.uint32)
+    dist = np.empty((nq, k), dtype=np.float64)
+    rc = lib().po_host_knn(_p(x), n, d, qp, nq if queries is not None else 0, k, _p(ids), _p(dist),
+                           _threads(threads))
+    if rc:
+        raise ValueError(f"po_host_knn failed ({rc})")
+    return ids, dist
+
+
+def host_build_nsg(base, k, R, threads=0):
+    """po_build_nsg's graph, built with cluster lower bounds (seconds at 1M):
+    returns (NSGGraph, knn ids n x k)."""
+    from parallel_anns_b200.formats import NSGGraph
+    x = np.ascontiguousarray(base, dtype=np.float32)
+    n, d = x.shape
+    knn = np.empty((n, k), dtype=np.uint32)
+    off = np.empty(n + 1, dtype=np.uint64)
+    cap = n * R + n
+    nbrs = np.empty(cap, dtype=np.uint32)
+    entry = np.zeros(1, dtype=np.uint32)
+    width = np.zeros(1, dtype=np.uint32)
+    rc = lib().po_host_build_nsg(_p(x), n, d, k, R, _p(knn), _p(entry), _p(off), _p(nbrs), cap, _p(width),
+                                 _threads(threads))
+    if rc:
+        raise ValueError(f"po_host_build_nsg failed ({rc})")
     g = NSGGraph(int(width[0]), int(entry[0]), off.astype(np.int64), nbrs[:int(off[-1])].copy())
     return g, knn

@@ -96,6 +96,16 @@ int po_build_nsg(const float *x, uint32_t n, uint32_t d, uint32_t k, uint32_t R,
                  uint32_t *entry_out, uint64_t *off_out, uint32_t *nbrs_out, uint64_t nbrs_cap,
                  uint32_t *width_out, int threads);
 
+/* The same graph as po_build_nsg and the same top-k as a float64 brute force
+ * (d64 by one FMA chain, ties by id), computed with cluster lower bounds so a
+ * 1M-vertex workload takes seconds (oracle/host_build.c). queries == NULL:
+ * the k-NN of every base row, the row itself excluded. */
+int po_host_knn(const float *x, uint32_t n, uint32_t d, const float *queries, uint32_t nq, uint32_t k,
+                uint32_t *out_ids, double *out_dist, int threads);
+int po_host_build_nsg(const float *x, uint32_t n, uint32_t d, uint32_t k, uint32_t R, uint32_t *knn_out,
+                      uint32_t *entry_out, uint64_t *off_out, uint32_t *nbrs_out, uint64_t nbrs_cap,
+                      uint32_t *width_out, int threads);
+
 #ifdef __cplusplus
 }
 #endif

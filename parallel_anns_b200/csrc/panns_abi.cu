@@ -526,27 +526,38 @@ int panns_info(const panns_index *h, uint32_t *n, uint32_t *d, uint32_t *nq, uin
     return PANNS_OK;
 }
 
-int panns_prepare_init_ids(const panns_index *h, uint32_t L, uint32_t *out) {
-    if (!h || !out) return fail(PANNS_EINVAL, "panns_prepare_init_ids: NULL argument");
-    if (!h->gn) return fail(PANNS_ESTATE, "panns_prepare_init_ids: no graph loaded");
+}  // extern "C"
+
+// The PANNS init list (prepare_init_ids, PSS.cpp:238-291): the entry's
+// neighbours in row order, each once, then entry + 1, entry + 2, ... (wrapping
+// at N), skipping the ones already taken. Only entry neighbours can repeat, so
+// a scan of the first part replaces a visited array: no allocation, which the
+// allocation-free search relies on.
+static void fill_init_ids(const panns_index *h, uint32_t L, uint32_t *out) {
     const uint32_t n = h->gn;
-    if (L == 0 || L > n) return fail(PANNS_EINVAL, "panns_prepare_init_ids: need 0 < L <= N");
-    std::vector<uint8_t> sel(n, 0);
     uint32_t end = 0;
     for (uint64_t e = h->off[h->entry]; e < h->off[h->entry + 1] && end < L; ++e) {
         const uint32_t v = h->nbrs[e];
-        if (sel[v]) continue;
-        sel[v] = 1;
-        out[end++] = v;
+        bool dup = false;
+        for (uint32_t i = 0; i < end && !dup; ++i) dup = out[i] == v;
+        if (!dup) out[end++] = v;
     }
-    uint32_t t = h->entry + 1;
-    while (end < L) {
+    const uint32_t from_nbrs = end;
+    for (uint32_t t = h->entry + 1; end < L; ++t) {
         if (t == n) t = 0;
-        const uint32_t v = t++;
-        if (sel[v]) continue;
-        sel[v] = 1;
-        out[end++] = v;
+        bool dup = false;
+        for (uint32_t i = 0; i < from_nbrs && !dup; ++i) dup = out[i] == t;
+        if (!dup) out[end++] = t;
     }
+}
+
+extern "C" {
+
+int panns_prepare_init_ids(const panns_index *h, uint32_t L, uint32_t *out) {
+    if (!h || !out) return fail(PANNS_EINVAL, "panns_prepare_init_ids: NULL argument");
+    if (!h->gn) return fail(PANNS_ESTATE, "panns_prepare_init_ids: no graph loaded");
+    if (L == 0 || L > h->gn) return fail(PANNS_EINVAL, "panns_prepare_init_ids: need 0 < L <= N");
+    fill_init_ids(h, L, out);
     return PANNS_OK;
 }
 
@@ -1278,7 +1289,9 @@ int panns_load_true_nn(const char *path, uint32_t *nq, uint32_t *K, uint32_t *id
 // that array until the process exits.
 //
 // The first call on a device looks up the array's device address
-// (cudaGetSymbolAddress); make that first call before any stream capture.
+// (cudaGetSymbolAddress). No call may be made while a stream is being
+// captured: every call copies the init list from host memory, reads the
+// error word back and synchronises its stream before it returns.
 // All calls share the array and it keeps the last call's contents: each call
 // zeroes what must start at zero. Calls that overlap on the GPU (from two
 // threads, or on two streams) race on the array and must not be made.
@@ -1333,6 +1346,9 @@ extern "C" int panns_search_static(panns_index *h, const panns_search_params *p,
         return fail(PANNS_EINVAL, "panns_search_static: TOP_M needs 1 <= M <= 64");
     if (p->warps_per_block > 8 || p->flags || p->storage != PANNS_STORE_FP32 || p->L_query)
         return fail(PANNS_EINVAL, "panns_search_static: bad params (float32 storage, no flags, no L_query)");
+    if (p->warps_per_query > 1 || p->blocks_per_sm)
+        return fail(PANNS_EINVAL, "panns_search_static: runs one warp per query with as many blocks per SM "
+                                  "as fit (warps_per_query <= 1, blocks_per_sm = 0)");
     if (nq == 0) return PANNS_OK;
     if (!d_queries || !d_out_ids) return fail(PANNS_EINVAL, "panns_search_static: NULL device buffer");
     cudaStream_t st = stream ? (cudaStream_t) stream : h->stream;
@@ -1381,24 +1397,11 @@ extern "C" int panns_search_static(panns_index *h, const panns_search_params *p,
                                       " leaves room for fewer than one block of warps in the fixed scratch");
     const uint32_t slots = blocks * wpb;
 
-    // Init ids (the PANNS list: entry's neighbours deduplicated, then entry+1,
-    // entry+2, ...), as device ids, built in a stack buffer.
+    // Init ids: the PANNS list (fill_init_ids, shared with
+    // panns_prepare_init_ids), as device ids, built in a stack buffer.
     uint32_t init[kStaticMaxL];
-    uint32_t end = 0;
-    const uint64_t e0 = h->off[h->entry], e1 = h->off[h->entry + 1];
-    for (uint64_t e = e0; e < e1 && end < p->L; ++e) {
-        const uint32_t v = h->nbrs[e];
-        bool dup = false;
-        for (uint32_t i = 0; i < end && !dup; ++i) dup = init[i] == v;
-        if (!dup) init[end++] = v;
-    }
-    const uint32_t from_nbrs = end;
-    for (uint32_t t = h->entry + 1; end < p->L; ++t) {
-        if (t == h->n) t = 0;
-        bool dup = false;
-        for (uint32_t i = 0; i < from_nbrs && !dup; ++i) dup = init[i] == t;
-        if (!dup) init[end++] = t;
-    }
+    const uint32_t end = p->L;
+    fill_init_ids(h, end, init);
     for (uint32_t i = 0; i < end; ++i) init[i] = h->inv[init[i]];
 
     uint32_t *counter = reinterpret_cast<uint32_t *>(base);

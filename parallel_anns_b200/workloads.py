@@ -67,15 +67,19 @@ def paths(spec):
                  truenn="truenn.bin", meta="meta.json").items()}
 
 
+def cached(spec) -> bool:
+    """True when the cache holds this exact workload."""
+    p = paths(spec)
+    if not os.path.exists(p["meta"]):
+        return False
+    with open(p["meta"]) as f:
+        return json.load(f).get("spec") == spec
+
+
 def build(spec, device=None, log=print):
     """Build (or load from the cache) a workload; returns a dict of arrays + paths."""
-    p = paths(spec)
-    if os.path.exists(p["meta"]):
-        with open(p["meta"]) as f:
-            meta = json.load(f)
-        if meta.get("spec") == spec:
-            return load(spec)
-    os.makedirs(p["root"], exist_ok=True)
+    if cached(spec):
+        return load(spec)
     t0 = time.time()
     base = vectors(spec, spec["n"], spec["base_seed"])
     q = vectors(spec, spec["nq"], spec["query_seed"])
@@ -84,15 +88,27 @@ def build(spec, device=None, log=print):
     t2 = time.time()
     gt_ids, gt_d = ground_truth(base, g, q, spec["gt_k"], device)
     t3 = time.time()
+    import torch
+    built_by = "gpu (graph_build.cu, gt_kernel.cuh)" if torch.cuda.is_available() else "torch on the host"
+    return store(spec, base, q, g, gt_ids, gt_d, built_by,
+                 {"generate": t1 - t0, "graph": t2 - t1, "ground_truth": t3 - t2}, log=log)
+
+
+def store(spec, base, q, g, gt_ids, gt_d, built_by, build_s, log=print):
+    """Write a built workload to the cache in the reference's formats (fvecs,
+    .nsg, true-NN) with its meta record; returns the workload dict."""
+    p = paths(spec)
+    os.makedirs(p["root"], exist_ok=True)
     fm.write_fvecs(p["base"], base)
     fm.write_fvecs(p["query"], q)
     fm.write_nsg(p["graph"], g)
-    fm.write_true_nn(p["truenn"], gt_ids, gt_d.astype(np.float32))
+    fm.write_true_nn(p["truenn"], gt_ids, np.asarray(gt_d).astype(np.float32))
     meta = {"spec": spec, "width": g.width, "entry": g.entry, "avg_degree": float(g.nbrs.size / g.n),
-            "build_s": {"generate": t1 - t0, "graph": t2 - t1, "ground_truth": t3 - t2}}
+            "built_by": built_by, "build_s": build_s}
     with open(p["meta"], "w") as f:
         json.dump(meta, f)
-    log(f"workload {spec['name']}: built in {time.time() - t0:.1f}s {meta['build_s']}")
+    if log:
+        log(f"workload {spec['name']}: built by {built_by} in {sum(build_s.values()):.1f}s {build_s}")
     return {"base": base, "queries": q, "graph": g, "gt": gt_ids, "paths": p, "meta": meta}
 
 
