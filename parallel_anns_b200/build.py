@@ -46,11 +46,14 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(p) <= t for p in DEPS if os.path.exists(p))
 
 
-def build(force: bool = False, verbose: bool = False, extra=None) -> str:
-    """Compile every source to an object in parallel, then link the shared library."""
-    if not force and up_to_date():
+def build(force: bool = False, verbose: bool = False, extra=None, out: str | None = None,
+          objdir: str | None = None) -> str:
+    """Compile every source to an object in parallel, then link the shared
+    library (``out``, default the in-tree library; ``objdir`` for the objects)."""
+    so = out or SO
+    if not force and out is None and up_to_date():
         return SO
-    objdir = os.path.join(PKG, "_build")
+    objdir = objdir or os.path.join(PKG, "_build")
     os.makedirs(objdir, exist_ok=True)
     procs = []
     objs = []
@@ -64,14 +67,17 @@ def build(force: bool = False, verbose: bool = False, extra=None) -> str:
     for cmd, p in procs:
         if p.wait() != 0:
             raise subprocess.CalledProcessError(p.returncode, cmd)
-    link = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", SO + ".tmp"] + objs + [
+    link = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", so + ".tmp"] + objs + [
         "-lcudart", "-lcublas"]
     subprocess.run(link, check=True, cwd=PKG)
-    os.replace(SO + ".tmp", SO)
-    return SO
+    os.replace(so + ".tmp", so)
+    return so
 
 
 if __name__ == "__main__":
     v = "-v" in sys.argv
-    extra = ["-Xptxas", "-v"] if "--ptxas" in sys.argv else None
-    print(build(force=True, verbose=v, extra=extra))
+    extra = ["-Xptxas", "-v"] if "--ptxas" in sys.argv else []
+    extra += [a for a in sys.argv[1:] if a.startswith("-D")]
+    out = next((a.split("=", 1)[1] for a in sys.argv[1:] if a.startswith("--out=")), None)
+    objdir = (out + ".objs") if out else None
+    print(build(force=True, verbose=v, extra=extra or None, out=out, objdir=objdir))

@@ -43,6 +43,7 @@
 // went from zero to non-zero, so only those are cleared after the query.
 #pragma once
 
+#include <cuda_fp16.h>
 #include <cuda_fp8.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -61,6 +62,9 @@ constexpr int kHeadNbrs = kHeadWords - 1;
 #endif
 #ifndef PANNS_WIDE_DIST
 #define PANNS_WIDE_DIST 0  // 1: 16 rows in flight per warp pass in the one-warp kernel too
+#endif
+#ifndef PANNS_FP8_MIXED
+#define PANNS_FP8_MIXED 0  // 1: FP8 rows times a half-precision query by mixed-precision FMAs
 #endif
 #ifndef PANNS_SEARCH_MIN_BLOCKS
 #define PANNS_SEARCH_MIN_BLOCKS 6
@@ -353,6 +357,105 @@ __device__ void warp_sort(float *bd, uint32_t *bi, uint32_t *bk, uint32_t cnt,
     }
 }
 
+#ifndef PANNS_MERGE_PATH
+#define PANNS_MERGE_PATH 0  // 1: merge by per-lane runs on the merge path (below)
+#endif
+#if PANNS_MERGE_PATH
+// Does the fresh element (fd, fid) precede the queue element (qdv, qid) in
+// the merged order? PANNS: (dist, original id); EFANNA: distance only, the
+// queue's (older) element first on equal distances. Ids may carry the
+// checked bit.
+template <int ORDER>
+__device__ __forceinline__ bool fresh_before(float fd, uint32_t fid, float qdv, uint32_t qid,
+                                             const uint32_t *__restrict__ orig) {
+    if (fd != qdv) return fd < qdv;
+    if (ORDER == ORDER_PANNS) return __ldg(orig + (fid & kIdMask)) < __ldg(orig + (qid & kIdMask));
+    return false;
+}
+
+#ifndef PANNS_MERGE_RUN
+#define PANNS_MERGE_RUN 4
+#endif
+constexpr uint32_t kMergeRun = PANNS_MERGE_RUN;
+
+// Merge the sorted fresh elements (bd, bi)[0..cnt) into the queue (qd, qi)
+// of size *sz and capacity cap (no id is in both). Returns the position of
+// the first fresh element if it was inserted (< cap), else cap.
+//
+// Only positions from p0 (the first fresh element's) on change. They are
+// produced from the back in rounds of 32 * kMergeRun: lane l finds where its
+// run of kMergeRun outputs starts on the merge path (a binary search over the
+// fresh elements), merges that run into registers, and the warp writes all
+// runs once every lane has read its inputs. A queue element only moves up,
+// so the positions a round writes are never read by a later (lower) round.
+template <int ORDER>
+__device__ uint32_t merge_into(float *qd, uint32_t *qi, uint32_t *sz, uint32_t cap, const float *bd,
+                               const uint32_t *bi, uint32_t *bk, uint32_t cnt, const uint32_t *orig,
+                               int lane) {
+    (void) bk;
+    const uint32_t qsz = *sz;
+    if (cnt == 0) return cap;
+    uint32_t p0;
+    {
+        const float f0 = bd[0];
+        const uint32_t g0 = bi[0];
+        uint32_t lo = 0, hi = qsz;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (fresh_before<ORDER>(f0, g0, qd[mid], qi[mid], orig)) hi = mid;
+            else lo = mid + 1;
+        }
+        p0 = lo;
+    }
+    if (p0 >= cap) return cap;
+    const uint32_t total = min(cap, qsz + cnt);
+    const uint32_t nA = qsz - p0;
+    for (int32_t hi_pos = (int32_t) total; hi_pos > (int32_t) p0; hi_pos -= 32 * (int32_t) kMergeRun) {
+        const int32_t s = hi_pos - 32 * (int32_t) kMergeRun + (int32_t) kMergeRun * lane;
+        const int32_t first = max(s, (int32_t) p0);
+        const int32_t last = min(s + (int32_t) kMergeRun, hi_pos);
+        float od[kMergeRun];
+        uint32_t oi[kMergeRun];
+        if (first < last) {
+            const uint32_t r = (uint32_t) first - p0;  // merged rank within the changed part
+            uint32_t lo = r > nA ? r - nA : 0u, hi = min(r, cnt);
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi) >> 1;
+                const uint32_t ia = p0 + (r - mid) - 1;
+                if (fresh_before<ORDER>(bd[mid], bi[mid], qd[ia], qi[ia], orig)) lo = mid + 1;
+                else hi = mid;
+            }
+            uint32_t j = lo, i = p0 + (r - lo);
+#pragma unroll
+            for (uint32_t t = 0; t < kMergeRun; ++t) {
+                if (first + (int32_t) t < last) {
+                    const bool take_f = j < cnt && (i >= qsz || fresh_before<ORDER>(bd[j], bi[j], qd[i], qi[i], orig));
+                    if (take_f) {
+                        od[t] = bd[j];
+                        oi[t] = bi[j];
+                        ++j;
+                    } else {
+                        od[t] = qd[i];
+                        oi[t] = qi[i];
+                        ++i;
+                    }
+                }
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (uint32_t t = 0; t < kMergeRun; ++t) {
+            if (first + (int32_t) t < last) {
+                qd[first + t] = od[t];
+                qi[first + t] = oi[t];
+            }
+        }
+        __syncwarp();
+    }
+    *sz = total;
+    return p0;
+}
+#else
 // Merge the sorted fresh elements (bd, bi)[0..cnt) into the queue (qd, qi)
 // of size *sz and capacity cap. Returns the position of the first fresh
 // element if it was inserted (< cap), else cap. Uses bk as scratch.
@@ -397,6 +500,8 @@ __device__ uint32_t merge_into(float *qd, uint32_t *qi, uint32_t *sz, uint32_t c
     *sz = min(cap, qsz + cnt);
     return p0;
 }
+
+#endif
 
 template <int ORDER>
 __device__ __forceinline__ uint32_t warp_merge(const WarpMem &m, uint32_t *sz, uint32_t L, uint32_t cnt,
@@ -513,7 +618,15 @@ static __device__ __forceinline__ int chain_major_pos(int d, int e) {
 // query once.
 template <int KIND, int CL, int STORE>
 struct Dist {
-    float ql[8 * CL];
+    // FP8 with PANNS_FP8_MIXED: the query (times the per-dimension scales and
+    // 2^12, which keeps it in half precision's normal range) as half pairs,
+    // multiplied with the E4M3 rows converted to half pairs by mixed-precision
+    // FMAs (half x half products are exact in float32, float32 accumulation);
+    // the 2^-12 is taken back in the final norm-trick FMA.
+    static constexpr bool kMixed = STORE == STORE_FP8 && PANNS_FP8_MIXED;
+    static constexpr float kMixedScale = 4096.0f;
+    float ql[kMixed ? 1 : 8 * CL];
+    uint32_t qh[kMixed ? 4 * CL : 1];
     __device__ __forceinline__ void load(const SearchArgs &a, uint32_t q, int lane) {
         const float *qrow = reinterpret_cast<const float *>(a.queries) + (size_t) q * (CL * 32);
         const int t = lane & 3;
@@ -524,12 +637,21 @@ struct Dist {
                 const int e = 8 * (t + 4 * i) + j;
                 float x = e < (int) a.d ? __ldg(qrow + chain_major_pos((int) a.d, e)) : 0.f;
                 if (STORE == STORE_FP8) x *= __ldg(a.scales + e);
-                ql[8 * i + j] = x;
+                if constexpr (kMixed) {
+                    const __half h = __float2half_rn(x * kMixedScale);
+                    const uint32_t hb = (uint32_t) __half_as_ushort(h);
+                    if (j & 1) qh[4 * i + j / 2] |= hb << 16;
+                    else qh[4 * i + j / 2] = hb;
+                } else {
+                    ql[8 * i + j] = x;
+                }
             }
         }
     }
-    __device__ __forceinline__ float dot_row(const void *vec_lo, uint32_t v, int t) const {
-        float acc = 0.f;
+    // Partial dot product of this lane's chunks of row v: component 0 sums
+    // the even elements, component 1 the odd ones (packed FMAs).
+    __device__ __forceinline__ float2 dot_row2(const void *vec_lo, uint32_t v, int t) const {
+        float2 acc = make_float2(0.f, 0.f);
         if (STORE == STORE_BF16) {
             const uint4 *row = reinterpret_cast<const uint4 *>(vec_lo) + (size_t) v * (CL * 4);
             uint4 x[CL];
@@ -540,8 +662,33 @@ struct Dist {
                 const uint32_t w[4] = {x[i].x, x[i].y, x[i].z, x[i].w};
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
-                    acc = fmaf(__uint_as_float(w[j] << 16), ql[8 * i + 2 * j], acc);
-                    acc = fmaf(__uint_as_float(w[j] & 0xffff0000u), ql[8 * i + 2 * j + 1], acc);
+                    acc.x = fmaf(__uint_as_float(w[j] << 16), ql[8 * i + 2 * j], acc.x);
+                    acc.x = fmaf(__uint_as_float(w[j] & 0xffff0000u), ql[8 * i + 2 * j + 1], acc.x);
+                }
+            }
+        } else if constexpr (kMixed) {
+            const uint2 *row = reinterpret_cast<const uint2 *>(vec_lo) + (size_t) v * (CL * 4);
+            uint2 x[CL];
+#pragma unroll
+            for (int i = 0; i < CL; ++i) x[i] = __ldg(row + t + 4 * i);
+#pragma unroll
+            for (int i = 0; i < CL; ++i) {
+                const uint32_t w[2] = {x[i].x, x[i].y};
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const __nv_fp8x2_storage_t pair = (__nv_fp8x2_storage_t) (w[j] >> (16 * h));
+                        const __half2_raw hr = __nv_cvt_fp8x2_to_halfraw2(pair, __NV_E4M3);
+                        const uint32_t xv = (uint32_t) hr.x | ((uint32_t) hr.y << 16);
+                        asm("{\n\t.reg .b16 a0, a1, b0, b1;\n\t"
+                            "mov.b32 {a0, a1}, %2;\n\t"
+                            "mov.b32 {b0, b1}, %3;\n\t"
+                            "fma.rn.f32.f16 %0, a0, b0, %0;\n\t"
+                            "fma.rn.f32.f16 %1, a1, b1, %1;\n\t}"
+                            : "+f"(acc.x), "+f"(acc.y)
+                            : "r"(xv), "r"(qh[4 * i + 2 * j + h]));
+                    }
                 }
             }
         } else {
@@ -559,8 +706,8 @@ struct Dist {
                         const __nv_fp8x2_storage_t pair = (__nv_fp8x2_storage_t) (w[j] >> (16 * h));
                         const __half2_raw hr = __nv_cvt_fp8x2_to_halfraw2(pair, __NV_E4M3);
                         const float2 f = __half22float2(*reinterpret_cast<const __half2 *>(&hr));
-                        acc = fmaf(f.x, ql[8 * i + 4 * j + 2 * h], acc);
-                        acc = fmaf(f.y, ql[8 * i + 4 * j + 2 * h + 1], acc);
+                        acc = __ffma2_rn(f, make_float2(ql[8 * i + 4 * j + 2 * h], ql[8 * i + 4 * j + 2 * h + 1]),
+                                         acc);
                     }
                 }
             }
@@ -575,17 +722,18 @@ struct Dist {
             const uint32_t b = b0 + g, bb = b0 + 8 + g;
             const bool act0 = b < nb, act1 = bb < nb;
             const uint32_t v0 = act0 ? ids[b] & kIdMask : 0u, v1 = act1 ? ids[bb] & kIdMask : 0u;
-            float s0 = act0 ? dot_row(a.vec_lo, v0, t) : 0.f;
-            float s1 = act1 ? dot_row(a.vec_lo, v1, t) : 0.f;
+            const float2 p0 = act0 ? dot_row2(a.vec_lo, v0, t) : make_float2(0.f, 0.f);
+            const float2 p1 = act1 ? dot_row2(a.vec_lo, v1, t) : make_float2(0.f, 0.f);
             const float n0 = act0 ? __ldg(a.norms_lo + v0) : 0.f;
             const float n1 = act1 ? __ldg(a.norms_lo + v1) : 0.f;
-            s0 += __shfl_xor_sync(kFull, s0, 1);
-            s1 += __shfl_xor_sync(kFull, s1, 1);
-            s0 += __shfl_xor_sync(kFull, s0, 2);
-            s1 += __shfl_xor_sync(kFull, s1, 2);
+            float2 s = __fadd2_rn(make_float2(p0.x, p1.x), make_float2(p0.y, p1.y));
+            s = __fadd2_rn(s, make_float2(__shfl_xor_sync(kFull, s.x, 1), __shfl_xor_sync(kFull, s.y, 1)));
+            s = __fadd2_rn(s, make_float2(__shfl_xor_sync(kFull, s.x, 2), __shfl_xor_sync(kFull, s.y, 2)));
             if (t == 0) {
-                if (act0) out[b] = fmaf(-2.f, s0, n0);
-                if (act1) out[bb] = fmaf(-2.f, s1, n1);
+                const float m2 = kMixed ? -2.f / kMixedScale : -2.f;
+                const float2 r = __ffma2_rn(make_float2(m2, m2), s, make_float2(n0, n1));
+                if (act0) out[b] = r.x;
+                if (act1) out[bb] = r.y;
             }
         }
         __syncwarp();
