@@ -848,12 +848,21 @@ static int launch_search(panns_index *h, const panns_search_params *p, float *d_
     uint32_t blocks = (uint32_t) per_sm * (uint32_t) h->num_sms;
     const uint32_t need_blocks = (nq + qpb - 1) / qpb;
     blocks = std::max(1u, std::min(blocks, need_blocks));
-    // Per-slot visited bitsets (bounded to 16 GiB) and dirty-word lists.
+    // Per-slot visited bitsets and dirty-word lists. When they must grow, they
+    // may take what they already hold plus half of the device's free memory
+    // (at least 1 GiB): at N = 100M a slot is 12.5 MB, and the 3,552 resident
+    // warps of a 148-SM part need 44 GB, which a 180 GB B200 holding the
+    // 100M index (about 77 GB) still has.
     const uint32_t vis_words = (h->n + 31) / 32;
     const uint32_t dirty_cap = 8192;
-    if ((uint64_t) blocks * qpb * vis_words * 4 > (16ull << 30)) {
-        const uint32_t max_slots = (uint32_t) ((16ull << 30) / (vis_words * 4ull));
-        blocks = std::max(1u, max_slots / qpb);
+    const uint64_t per_slot = ((uint64_t) vis_words + dirty_cap) * 4;
+    if ((uint64_t) blocks * qpb > h->vis_slots || h->vis_words != vis_words) {
+        size_t free_b = 0, total_b = 0;
+        CU(cudaMemGetInfo(&free_b, &total_b));
+        const uint64_t held = ((uint64_t) h->visited.n + h->dirty.n) * 4;
+        const uint64_t budget = std::max<uint64_t>(1ull << 30, held + free_b / 2);
+        const uint64_t max_slots = budget / per_slot;
+        if ((uint64_t) blocks * qpb > max_slots) blocks = (uint32_t) std::max<uint64_t>(1, max_slots / qpb);
     }
     const uint32_t nslots = blocks * qpb;
     if (h->vis_slots < nslots || h->vis_words != vis_words) {

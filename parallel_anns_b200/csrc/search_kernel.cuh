@@ -64,7 +64,7 @@ constexpr int kHeadNbrs = kHeadWords - 1;
 #define PANNS_WIDE_DIST 0  // 1: 16 rows in flight per warp pass in the one-warp kernel too
 #endif
 #ifndef PANNS_FP8_MIXED
-#define PANNS_FP8_MIXED 0  // 1: FP8 rows times a half-precision query by mixed-precision FMAs
+#define PANNS_FP8_MIXED 1  // FP8 rows times a half-precision query by mixed-precision FMAs
 #endif
 #ifndef PANNS_SEARCH_MIN_BLOCKS
 #define PANNS_SEARCH_MIN_BLOCKS 6
@@ -357,105 +357,6 @@ __device__ void warp_sort(float *bd, uint32_t *bi, uint32_t *bk, uint32_t cnt,
     }
 }
 
-#ifndef PANNS_MERGE_PATH
-#define PANNS_MERGE_PATH 0  // 1: merge by per-lane runs on the merge path (below)
-#endif
-#if PANNS_MERGE_PATH
-// Does the fresh element (fd, fid) precede the queue element (qdv, qid) in
-// the merged order? PANNS: (dist, original id); EFANNA: distance only, the
-// queue's (older) element first on equal distances. Ids may carry the
-// checked bit.
-template <int ORDER>
-__device__ __forceinline__ bool fresh_before(float fd, uint32_t fid, float qdv, uint32_t qid,
-                                             const uint32_t *__restrict__ orig) {
-    if (fd != qdv) return fd < qdv;
-    if (ORDER == ORDER_PANNS) return __ldg(orig + (fid & kIdMask)) < __ldg(orig + (qid & kIdMask));
-    return false;
-}
-
-#ifndef PANNS_MERGE_RUN
-#define PANNS_MERGE_RUN 4
-#endif
-constexpr uint32_t kMergeRun = PANNS_MERGE_RUN;
-
-// Merge the sorted fresh elements (bd, bi)[0..cnt) into the queue (qd, qi)
-// of size *sz and capacity cap (no id is in both). Returns the position of
-// the first fresh element if it was inserted (< cap), else cap.
-//
-// Only positions from p0 (the first fresh element's) on change. They are
-// produced from the back in rounds of 32 * kMergeRun: lane l finds where its
-// run of kMergeRun outputs starts on the merge path (a binary search over the
-// fresh elements), merges that run into registers, and the warp writes all
-// runs once every lane has read its inputs. A queue element only moves up,
-// so the positions a round writes are never read by a later (lower) round.
-template <int ORDER>
-__device__ uint32_t merge_into(float *qd, uint32_t *qi, uint32_t *sz, uint32_t cap, const float *bd,
-                               const uint32_t *bi, uint32_t *bk, uint32_t cnt, const uint32_t *orig,
-                               int lane) {
-    (void) bk;
-    const uint32_t qsz = *sz;
-    if (cnt == 0) return cap;
-    uint32_t p0;
-    {
-        const float f0 = bd[0];
-        const uint32_t g0 = bi[0];
-        uint32_t lo = 0, hi = qsz;
-        while (lo < hi) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (fresh_before<ORDER>(f0, g0, qd[mid], qi[mid], orig)) hi = mid;
-            else lo = mid + 1;
-        }
-        p0 = lo;
-    }
-    if (p0 >= cap) return cap;
-    const uint32_t total = min(cap, qsz + cnt);
-    const uint32_t nA = qsz - p0;
-    for (int32_t hi_pos = (int32_t) total; hi_pos > (int32_t) p0; hi_pos -= 32 * (int32_t) kMergeRun) {
-        const int32_t s = hi_pos - 32 * (int32_t) kMergeRun + (int32_t) kMergeRun * lane;
-        const int32_t first = max(s, (int32_t) p0);
-        const int32_t last = min(s + (int32_t) kMergeRun, hi_pos);
-        float od[kMergeRun];
-        uint32_t oi[kMergeRun];
-        if (first < last) {
-            const uint32_t r = (uint32_t) first - p0;  // merged rank within the changed part
-            uint32_t lo = r > nA ? r - nA : 0u, hi = min(r, cnt);
-            while (lo < hi) {
-                const uint32_t mid = (lo + hi) >> 1;
-                const uint32_t ia = p0 + (r - mid) - 1;
-                if (fresh_before<ORDER>(bd[mid], bi[mid], qd[ia], qi[ia], orig)) lo = mid + 1;
-                else hi = mid;
-            }
-            uint32_t j = lo, i = p0 + (r - lo);
-#pragma unroll
-            for (uint32_t t = 0; t < kMergeRun; ++t) {
-                if (first + (int32_t) t < last) {
-                    const bool take_f = j < cnt && (i >= qsz || fresh_before<ORDER>(bd[j], bi[j], qd[i], qi[i], orig));
-                    if (take_f) {
-                        od[t] = bd[j];
-                        oi[t] = bi[j];
-                        ++j;
-                    } else {
-                        od[t] = qd[i];
-                        oi[t] = qi[i];
-                        ++i;
-                    }
-                }
-            }
-        }
-        __syncwarp();
-#pragma unroll
-        for (uint32_t t = 0; t < kMergeRun; ++t) {
-            if (first + (int32_t) t < last) {
-                qd[first + t] = od[t];
-                qi[first + t] = oi[t];
-            }
-        }
-        __syncwarp();
-    }
-    *sz = total;
-    return p0;
-}
-#else
 // Merge the sorted fresh elements (bd, bi)[0..cnt) into the queue (qd, qi)
 // of size *sz and capacity cap. Returns the position of the first fresh
 // element if it was inserted (< cap), else cap. Uses bk as scratch.
@@ -500,8 +401,6 @@ __device__ uint32_t merge_into(float *qd, uint32_t *qi, uint32_t *sz, uint32_t c
     *sz = min(cap, qsz + cnt);
     return p0;
 }
-
-#endif
 
 template <int ORDER>
 __device__ __forceinline__ uint32_t warp_merge(const WarpMem &m, uint32_t *sz, uint32_t L, uint32_t cnt,
@@ -648,25 +547,29 @@ struct Dist {
             }
         }
     }
-    // Partial dot product of this lane's chunks of row v: component 0 sums
-    // the even elements, component 1 the odd ones (packed FMAs).
+    // BF16: partial dot product of this lane's chunks of row v.
+    __device__ __forceinline__ float dot_row_bf16(const void *vec_lo, uint32_t v, int t) const {
+        float acc = 0.f;
+        const uint4 *row = reinterpret_cast<const uint4 *>(vec_lo) + (size_t) v * (CL * 4);
+        uint4 x[CL];
+#pragma unroll
+        for (int i = 0; i < CL; ++i) x[i] = __ldg(row + t + 4 * i);
+#pragma unroll
+        for (int i = 0; i < CL; ++i) {
+            const uint32_t w[4] = {x[i].x, x[i].y, x[i].z, x[i].w};
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                acc = fmaf(__uint_as_float(w[j] << 16), ql[8 * i + 2 * j], acc);
+                acc = fmaf(__uint_as_float(w[j] & 0xffff0000u), ql[8 * i + 2 * j + 1], acc);
+            }
+        }
+        return acc;
+    }
+    // FP8: partial dot product of this lane's chunks of row v, component 0
+    // over the even elements, component 1 over the odd ones.
     __device__ __forceinline__ float2 dot_row2(const void *vec_lo, uint32_t v, int t) const {
         float2 acc = make_float2(0.f, 0.f);
-        if (STORE == STORE_BF16) {
-            const uint4 *row = reinterpret_cast<const uint4 *>(vec_lo) + (size_t) v * (CL * 4);
-            uint4 x[CL];
-#pragma unroll
-            for (int i = 0; i < CL; ++i) x[i] = __ldg(row + t + 4 * i);
-#pragma unroll
-            for (int i = 0; i < CL; ++i) {
-                const uint32_t w[4] = {x[i].x, x[i].y, x[i].z, x[i].w};
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    acc.x = fmaf(__uint_as_float(w[j] << 16), ql[8 * i + 2 * j], acc.x);
-                    acc.x = fmaf(__uint_as_float(w[j] & 0xffff0000u), ql[8 * i + 2 * j + 1], acc.x);
-                }
-            }
-        } else if constexpr (kMixed) {
+        if constexpr (kMixed) {
             const uint2 *row = reinterpret_cast<const uint2 *>(vec_lo) + (size_t) v * (CL * 4);
             uint2 x[CL];
 #pragma unroll
@@ -722,10 +625,23 @@ struct Dist {
             const uint32_t b = b0 + g, bb = b0 + 8 + g;
             const bool act0 = b < nb, act1 = bb < nb;
             const uint32_t v0 = act0 ? ids[b] & kIdMask : 0u, v1 = act1 ? ids[bb] & kIdMask : 0u;
-            const float2 p0 = act0 ? dot_row2(a.vec_lo, v0, t) : make_float2(0.f, 0.f);
-            const float2 p1 = act1 ? dot_row2(a.vec_lo, v1, t) : make_float2(0.f, 0.f);
             const float n0 = act0 ? __ldg(a.norms_lo + v0) : 0.f;
             const float n1 = act1 ? __ldg(a.norms_lo + v1) : 0.f;
+            if constexpr (STORE == STORE_BF16) {
+                float s0 = act0 ? dot_row_bf16(a.vec_lo, v0, t) : 0.f;
+                float s1 = act1 ? dot_row_bf16(a.vec_lo, v1, t) : 0.f;
+                s0 += __shfl_xor_sync(kFull, s0, 1);
+                s1 += __shfl_xor_sync(kFull, s1, 1);
+                s0 += __shfl_xor_sync(kFull, s0, 2);
+                s1 += __shfl_xor_sync(kFull, s1, 2);
+                if (t == 0) {
+                    if (act0) out[b] = fmaf(-2.f, s0, n0);
+                    if (act1) out[bb] = fmaf(-2.f, s1, n1);
+                }
+                continue;
+            }
+            const float2 p0 = act0 ? dot_row2(a.vec_lo, v0, t) : make_float2(0.f, 0.f);
+            const float2 p1 = act1 ? dot_row2(a.vec_lo, v1, t) : make_float2(0.f, 0.f);
             float2 s = __fadd2_rn(make_float2(p0.x, p1.x), make_float2(p0.y, p1.y));
             s = __fadd2_rn(s, make_float2(__shfl_xor_sync(kFull, s.x, 1), __shfl_xor_sync(kFull, s.y, 1)));
             s = __fadd2_rn(s, make_float2(__shfl_xor_sync(kFull, s.x, 2), __shfl_xor_sync(kFull, s.y, 2)));
