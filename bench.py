@@ -49,6 +49,14 @@ L_SWEEP = [100, 128, 160, 200, 256, 320, 400, 512, 640, 800]
 M_SWEEP = [1, 2, 4, 8, 16]
 
 
+def metric_for(spec):
+    """The metric's name for a workload (the default one is the name the
+    benchmark is quoted under)."""
+    if spec["n"] == 1_000_000 and spec["d"] == 96:
+        return METRIC
+    return METRIC.replace("1M x 96d", f"{spec['n'] / 1e6:g}M x {spec['d']}d")
+
+
 def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
@@ -256,7 +264,8 @@ def bench_ours(args):
     barrier = ranks.barrier
     max_over_ranks = ranks.max
 
-    spec = workloads.SPECS[args.workload](n=args.n, nq=args.nq * world)
+    spec = workloads.SPECS[args.workload](**({"n": args.n} if args.n else {}), nq=args.nq * world)
+    args.n = spec["n"]
     fixed = bool(args.L and args.M)  # a given operating point: no tuning set, no autotuning
     if rank == 0:
         W = workloads.build(spec, device=f"cuda:{local}", log=log)
@@ -495,7 +504,7 @@ def bench_ours(args):
         log("details " + json.dumps(details))
         # The JSON line stays short (the full tables go to stderr above).
         line = {
-            "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
+            "metric": metric_for(spec), "value": round(value, 1), "unit": UNIT, "n_gpus": world,
             "steps": steps, "warmup": args.warmup,
             "ms_per_step": round(kernel_ms_max / steps, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": names[store], "data": "synthetic",
@@ -577,7 +586,8 @@ def bench_reference(args):
         print(json.dumps({"impl": "reference", "unavailable":
                           "reference binaries were not built (oracle/_ref/ref_pss missing)"}))
         return
-    spec = workloads.SPECS[args.workload](n=args.n, nq=args.nq)
+    spec = workloads.SPECS[args.workload](**({"n": args.n} if args.n else {}), nq=args.nq)
+    args.n = spec["n"]
     # Inputs: the cached files if present, else built on the host (no GPU
     # library in this process).
     if workloads.cached(spec):
@@ -617,7 +627,7 @@ def bench_reference(args):
                           inner=inner)
     times = r["rep_times"][args.warmup:]
     value = sample * len(times) / sum(times)
-    line = {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
+    line = {"metric": metric_for(spec), "value": round(value, 1), "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(1e3 * sum(times) / len(times), 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -639,7 +649,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=1_000_000)
+    ap.add_argument("--n", type=int, default=None, help="base size (default: the workload's)")
     ap.add_argument("--nq", type=int, default=10_000, help="queries per GPU")
     ap.add_argument("--L", type=int, default=0, help="fix L (default: recall-driven sweep)")
     ap.add_argument("--M", type=int, default=0, help="fix M (default: sweep)")
@@ -649,9 +659,10 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="leave the learned entry network out")
     ap.add_argument("--no-parity", action="store_true", help="skip the id check against the reference")
     ap.add_argument("--wpb", type=int, default=2, help="warps per block with a fixed --L and --M")
-    ap.add_argument("--workload", default="mixture_1m_d96", choices=["mixture_1m_d96", "u8_1m_d128"],
+    ap.add_argument("--workload", default="mixture_1m_d96", choices=["mixture_1m_d96", "u8_1m_d128", "mixture_10m_d96"],
                     help="mixture_1m_d96: the batched-FP32 config (default); u8_1m_d128: the "
-                         "reduced-precision config's integer-valued d = 128 variant (R = 64)")
+                         "reduced-precision config's integer-valued d = 128 variant (R = 64); mixture_10m_d96: "
+                         "the learned-entry config's 10M base")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -29,12 +29,16 @@ extern "C" {
 typedef struct panns_graph panns_graph;
 
 /* k-NN screen of the build: all pairs in float32 on CUDA cores keeping k + 8
- * candidates per row, or by TF32 tensor-core GEMMs (cuBLAS) keeping k + 32;
- * either way the candidates are ranked exactly in float64. AUTO: TF32 from
- * 100,000 vectors on. */
+ * candidates per row; by TF32 tensor-core GEMMs (cuBLAS) keeping k + 32; or
+ * by the library's own tcgen05 kernel (TF32 MMAs into tensor memory, TMA-fed,
+ * the per-row selection in the epilogue, no distance tile written; d a
+ * multiple of 32 up to 128) keeping k + 32. Either way the candidates are
+ * ranked exactly in float64. AUTO: the tcgen05 kernel from 100,000 vectors on
+ * where it applies, else TF32 from 100,000 vectors on, else float32. */
 #define PANNS_SCREEN_AUTO 0u
 #define PANNS_SCREEN_FP32 1u
 #define PANNS_SCREEN_TF32 2u
+#define PANNS_SCREEN_TC 3u
 
 /* Build the graph of n row-major float32 vectors of width d (host pointer) on
  * GPU `device`; knn_k <= 128, 0 < R <= knn_k. *out is released with
@@ -59,6 +63,24 @@ int panns_graph_copy(const panns_graph *g, uint64_t *offsets, uint32_t *nbrs, ui
 int panns_graph_save_nsg(const panns_graph *g, const char *path);
 
 int panns_graph_free(panns_graph *g);
+
+/* efanna2e's own NSG construction, IndexNSG::Build
+ * (include/efanna2e/index_nsg.cpp:403-450; get_neighbors :141-207,
+ * sync_prune :226-276, InterInsert :278-354, tree_grow / DFS / findroot
+ * :638-718), with the reference's parameters L (search pool), R (degree) and
+ * C (candidates considered by the prune), from a k-NN graph given as
+ * n x knn_k ids (what IndexNSG::Load_nn_graph reads from an EFANNA file) and
+ * n row-major float32 vectors of width d (a multiple of 8), host pointers.
+ * The result equals the reference's Build run with one OpenMP thread from a
+ * glibc rand() stream seeded with rand_seed (1 = a process that never called
+ * srand): every vertex's search and prune runs on GPU `device`, one warp per
+ * vertex, the reverse-edge insertion and the reachability repair on the host
+ * in the reference's order. Exactly equal distances (duplicate rows) are the
+ * one input whose order the reference leaves unspecified. *out is released
+ * with panns_graph_free; panns_graph_save_nsg writes it as IndexNSG::Save. */
+int panns_efanna_build(int device, const float *base, uint32_t n, uint32_t d, const uint32_t *knn,
+                       uint32_t knn_k, uint32_t L, uint32_t R, uint32_t C, uint32_t rand_seed,
+                       panns_graph **out);
 
 #ifdef __cplusplus
 }

@@ -269,6 +269,30 @@ def ref_binary(name: str) -> str:
     return os.path.join(REF_DIR, name)
 
 
+def ref_nsg_build(base_path: str, knn_path: str, L: int, R: int, C: int, out_path: str, threads: int = 1):
+    """efanna2e IndexNSG::Build by the reference's tools/test_nsg_index.cpp
+    (oracle/_ref/ref_nsg_build) at `threads` OpenMP threads."""
+    args = [ref_binary("ref_nsg_build"), base_path, knn_path, str(L), str(R), str(C), out_path, str(threads)]
+    r = subprocess.run(args, check=True, capture_output=True, text=True)
+    return r.stdout
+
+
+def write_efanna_knn(path: str, knn: np.ndarray) -> None:
+    """An EFANNA k-NN graph file (what IndexNSG::Load_nn_graph reads): per
+    vertex u32 k, then k u32 ids."""
+    knn = np.ascontiguousarray(knn, dtype=np.uint32)
+    rec = np.empty((knn.shape[0], knn.shape[1] + 1), dtype=np.uint32)
+    rec[:, 0] = knn.shape[1]
+    rec[:, 1:] = knn
+    rec.tofile(path)
+
+
+def read_efanna_knn(path: str) -> np.ndarray:
+    raw = np.fromfile(path, dtype=np.uint32)
+    k = int(raw[0])
+    return raw.reshape(-1, k + 1)[:, 1:].copy()
+
+
 def have_ref() -> bool:
     return all(os.path.exists(ref_binary(b)) for b in ("ref_pss", "ref_pss_lg", "ref_topm", "ref_efanna"))
 

@@ -17,10 +17,10 @@ SO = os.path.join(PKG, "libpanns_b200.so")
 SOURCES = [os.path.join(PKG, "csrc", f) for f in
            ("panns_abi.cu", "search_kernels_fp32_ip.cu", "search_kernels_fp32_l2.cu",
             "search_kernels_bf16.cu", "search_kernels_fp8.cu", "pss_kernels.cu", "learned.cu", "graph_build.cu", "search_block_kernels_fp32.cu", "search_block_kernels_bf16.cu",
-            "search_block_kernels_fp8.cu")]
+            "search_block_kernels_fp8.cu", "nsg_build.cu", "tc_screen.cu")]
 DEPS = SOURCES + [os.path.join(PKG, "csrc", f) for f in
                   ("search_kernel.cuh", "pss_kernel.cuh", "gt_kernel.cuh", "kernels.h", "search_kernels.inc",
-                   "mlp_infer.cuh", "learned.h", "block_kernel.cuh")] + [
+                   "mlp_infer.cuh", "learned.h", "block_kernel.cuh", "graph_types.h", "tc_screen.h")] + [
     os.path.join(ROOT, "include", "panns_b200.h"), os.path.join(ROOT, "include", "panns_learned.h"),
     os.path.join(ROOT, "include", "panns_build.h"),
 ]

@@ -31,7 +31,9 @@
 #include <vector>
 
 #include "../../include/panns_build.h"
+#include "graph_types.h"
 #include "learned.h"
+#include "tc_screen.h"
 
 namespace panns {
 namespace {
@@ -319,15 +321,6 @@ __global__ void dist_to_point_kernel(const float *__restrict__ x, uint32_t n, ui
 }  // namespace
 }  // namespace panns
 
-struct panns_graph {
-    uint32_t n = 0, width = 0, entry = 0;
-    std::vector<uint64_t> off;
-    std::vector<uint32_t> nbrs;
-    std::vector<uint32_t> knn;  // n x k (kept for the repair and for callers)
-    uint32_t k = 0;
-    uint32_t repaired = 0;
-};
-
 using namespace panns;
 
 extern "C" {
@@ -345,11 +338,16 @@ int panns_build_nsg_ex(int device, const float *base, uint32_t n, uint32_t d, ui
     if (knn_k == 0 || knn_k >= n) return set_error(PANNS_EINVAL, "panns_build_nsg: need 0 < knn_k < n");
     if (knn_k + 8 > (uint32_t) kMaxC) return set_error(PANNS_EINVAL, "panns_build_nsg: knn_k > 128 is not supported");
     if (R == 0 || R > knn_k) return set_error(PANNS_EINVAL, "panns_build_nsg: need 0 < R <= knn_k");
-    if (screen > PANNS_SCREEN_TF32) return set_error(PANNS_EINVAL, "panns_build_nsg: unknown screen");
-    if (screen == PANNS_SCREEN_AUTO) screen = n >= 100000 ? PANNS_SCREEN_TF32 : PANNS_SCREEN_FP32;
-    const bool tc = screen == PANNS_SCREEN_TF32;
+    if (screen > PANNS_SCREEN_TC) return set_error(PANNS_EINVAL, "panns_build_nsg: unknown screen");
     const uint32_t k = knn_k;
-    const uint32_t C = std::min(std::min(knn_k + (tc ? 32u : 8u), (uint32_t) kMaxC), n - 1);
+    const uint32_t C_tc = std::min(std::min(knn_k + 32u, (uint32_t) kMaxC), n - 1);
+    if (screen == PANNS_SCREEN_AUTO) screen = n < 100000 ? PANNS_SCREEN_FP32 : PANNS_SCREEN_TF32;
+    if (screen == PANNS_SCREEN_TC && !tc_screen_supported(n, d, C_tc))
+        return set_error(PANNS_EINVAL, "panns_build_nsg: the tcgen05 screen needs d a multiple of 32 up to 128 "
+                                       "and n >= 128");
+    const bool tc = screen == PANNS_SCREEN_TF32;
+    const bool tcg = screen == PANNS_SCREEN_TC;
+    const uint32_t C = (tc || tcg) ? C_tc : std::min(std::min(knn_k + 8u, (uint32_t) kMaxC), n - 1);
     GCU(cudaSetDevice(device));
     cudaStream_t s = nullptr;
     GCU(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
@@ -371,7 +369,12 @@ int panns_build_nsg_ex(int device, const float *base, uint32_t n, uint32_t d, ui
     GCU(dm.alloc(n));
     GCU(cudaMemcpyAsync(x.p, base, (size_t) n * d * 4, cudaMemcpyHostToDevice, s));
     sqnorm32_kernel<<<(n + 255) / 256, 256, 0, s>>>(x.p, n, d, xn.p);
-    if (!tc) {
+    if (tcg) {
+        int num_sms = 0;
+        GCU(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device));
+        const int rc = tc_screen(x.p, xn.p, n, d, C, cand.p, num_sms, s);
+        if (rc) return rc;
+    } else if (!tc) {
         const size_t smem = (size_t) (kBK * kBQ + kBK * kBV + kBQ * (kBV + 1)) * 4 + (size_t) kBQ * C * 8 + kBQ * 4;
         GCU(cudaFuncSetAttribute(screen_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
         screen_kernel<<<(n + kBQ - 1) / kBQ, 256, smem, s>>>(x.p, n, d, xn.p, C, cand.p);

@@ -15,6 +15,7 @@
 
 #include "../../include/panns_b200.h"
 #include "../../include/panns_learned.h"
+#include "graph_types.h"
 #include "learned.h"
 #include "search_kernel.cuh"
 #include "block_kernel.cuh"
@@ -1568,3 +1569,21 @@ extern "C" int panns_learned_record(panns_index *h, uint32_t nq, uint32_t *out) 
     }
     return PANNS_OK;
 }
+
+int32_t panns::glibc_rand_next(int32_t *st) { return rand_next(st); }
+
+#ifdef PANNS_DEBUG_VISITED
+// Diagnostic builds only: the number of non-zero words left in the handle's
+// visited bitsets (zero between calls when every query cleared its bits).
+extern "C" int panns_debug_visited_nonzero(panns_index *h, uint64_t *count) {
+    if (!h || !count) return fail(PANNS_EINVAL, "NULL argument");
+    CU(cudaSetDevice(h->device));
+    CU(cudaDeviceSynchronize());
+    std::vector<uint32_t> v((size_t) h->vis_slots * h->vis_words);
+    if (!v.empty()) CU(cudaMemcpy(v.data(), h->visited.p, v.size() * 4, cudaMemcpyDeviceToHost));
+    uint64_t c = 0;
+    for (uint32_t w : v) c += w != 0;
+    *count = c;
+    return PANNS_OK;
+}
+#endif

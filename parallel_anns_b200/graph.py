@@ -11,7 +11,7 @@ from . import native as N
 from .formats import NSGGraph
 
 
-SCREEN_AUTO, SCREEN_FP32, SCREEN_TF32 = 0, 1, 2
+SCREEN_AUTO, SCREEN_FP32, SCREEN_TF32, SCREEN_TC = 0, 1, 2, 3
 
 
 def build_nsg(base: np.ndarray, R: int = 50, knn_k: int = 64, device: int = 0, with_knn: bool = False,
@@ -48,3 +48,26 @@ def save_nsg_gpu_built(base: np.ndarray, path: str, R: int = 50, knn_k: int = 64
         N.check(lib.panns_graph_save_nsg(g, path.encode()))
     finally:
         lib.panns_graph_free(g)
+
+
+def efanna_build(base: np.ndarray, knn: np.ndarray, L: int, R: int, C: int, rand_seed: int = 1,
+                 device: int = 0) -> NSGGraph:
+    """efanna2e's IndexNSG::Build from a k-NN graph (n x k ids), the result
+    equal to the reference's at one thread (include/panns_build.h)."""
+    x = np.ascontiguousarray(base, dtype=np.float32)
+    kn = np.ascontiguousarray(knn, dtype=np.uint32)
+    n, d = x.shape
+    lib = N.load()
+    g = ctypes.c_void_p()
+    N.check(lib.panns_efanna_build(device, N.ptr(x), n, d, N.ptr(kn), kn.shape[1], L, R, C, rand_seed,
+                                   ctypes.byref(g)))
+    try:
+        vals = [ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint64(), ctypes.c_uint32()]
+        N.check(lib.panns_graph_info(g, *[ctypes.byref(v) for v in vals]))
+        _, width, entry, n_edges, _ = [v.value for v in vals]
+        off = np.empty(n + 1, dtype=np.uint64)
+        nbrs = np.empty(max(n_edges, 1), dtype=np.uint32)
+        N.check(lib.panns_graph_copy(g, N.ptr(off), N.ptr(nbrs), None))
+    finally:
+        lib.panns_graph_free(g)
+    return NSGGraph(int(width), int(entry), off.astype(np.int64), nbrs[:n_edges].copy())

@@ -33,6 +33,7 @@ EXPORTS = [
     "panns_kmeans", "panns_set_learned", "panns_learned_record",
     # include/panns_build.h
     "panns_build_nsg", "panns_build_nsg_ex", "panns_graph_info", "panns_graph_copy", "panns_graph_save_nsg", "panns_graph_free",
+    "panns_efanna_build",
 ]
 
 
@@ -131,6 +132,7 @@ def load(build_if_missing: bool = True):
     L.panns_graph_copy.argtypes = [P, P, P, P]
     L.panns_graph_save_nsg.argtypes = [P, ctypes.c_char_p]
     L.panns_graph_free.argtypes = [P]
+    L.panns_efanna_build.argtypes = [i32, P, u32, u32, P, u32, u32, u32, u32, u32, ctypes.POINTER(P)]
     for name in EXPORTS:
         getattr(L, name).restype = getattr(L, name).restype or ctypes.c_int
     L.panns_last_error.restype = ctypes.c_char_p

@@ -38,7 +38,16 @@ def spec_u8_1m_d128(n=1_000_000, nq=10_000):
             "knn_k": 64, "base_seed": 1002, "query_seed": 2002, "gt_k": 100}
 
 
-SPECS = {"mixture_1m_d96": spec_batched_fp32_1m, "u8_1m_d128": spec_u8_1m_d128}
+def spec_mixture_10m_d96(n=10_000_000, nq=10_000):
+    """The learned-entry config's base: N = 10M, d = 96, the same mixture
+    generator (another seed), R = 50."""
+    return {"name": f"mixture64_n{n}_d96_q{nq}_R50", "n": n, "d": 96, "nq": nq, "R": 50,
+            "knn_k": 64, "components": 64, "sigma": 0.3, "base_seed": 1003, "query_seed": 2003,
+            "gt_k": 100}
+
+
+SPECS = {"mixture_1m_d96": spec_batched_fp32_1m, "u8_1m_d128": spec_u8_1m_d128,
+         "mixture_10m_d96": spec_mixture_10m_d96}
 
 
 def describe(spec) -> str:
