@@ -303,7 +303,10 @@ def bench_ours(args):
         barrier()
         if rank != 0:
             model = workloads.learned_model(spec, handles[N.STORE_BF16], log=None)
-    learned_opts = [dict(E=8, L_init=8, use_L=False), dict(E=32, L_init=0, use_L=False)]
+    # Learned options: entries with a few plain init ids kept, entries only, and
+    # entries with the plain search for queries the network is unsure of.
+    learned_opts = [dict(E=8, L_init=8, use_L=False), dict(E=32, L_init=0, use_L=False),
+                    dict(E=16, L_init=16, use_L=False, min_conf=0.5)]
 
     # Operating points, chosen by the autotuner on the tuning queries (not the
     # evaluated ones) on rank 0: the plain FP32 search, and the fastest of all

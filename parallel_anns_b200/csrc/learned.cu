@@ -51,10 +51,27 @@ struct Dev {
 __device__ __forceinline__ float to_f(float x) { return x; }
 __device__ __forceinline__ float to_f(__nv_bfloat16 x) { return __bfloat162float(x); }
 
+// TF32 split of x: hi = x rounded to TF32, lo = the remainder rounded to TF32.
+__device__ __forceinline__ void split_tf32(float x, uint32_t &hi, uint32_t &lo) {
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hi) : "f"(x));
+    const float r = x - __uint_as_float(hi);
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lo) : "f"(r));
+}
+
+// c += a * b for one m16n8k8 tile (A row-major, B column-major, TF32, float32 accumulate).
+__device__ __forceinline__ void mma_tf32(float (&c)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+        "{%0, %1, %2, %3};"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
 // C[M x N] = A(M x K) * B(K x N) (+ bias[n]) (relu) (or C += when accumulate).
 // A(m, k) = AT ? A[k * lda + m] : A[m * lda + k]; B(k, n) = BT ? B[n * ldb + k]
-// : B[k * ldb + n]. 64 x 64 tiles, 16-deep k steps, 4 x 4 outputs per thread;
-// the k order of every sum is fixed (deterministic).
+// : B[k * ldb + n]. 64 x 64 tiles staged through shared memory 16 deep, the
+// products on the tensor cores (split TF32, float32 accumulation); the order
+// of every sum is fixed, so results are deterministic.
 template <typename TA, typename TB, bool AT, bool BT>
 __global__ void __launch_bounds__(256) gemm_kernel(const TA *__restrict__ A, int lda, const TB *__restrict__ B,
                                                    int ldb, float *__restrict__ C, int ldc, int M, int N, int K,
@@ -63,7 +80,10 @@ __global__ void __launch_bounds__(256) gemm_kernel(const TA *__restrict__ A, int
     __shared__ float Bs[16][64 + 4];
     const int tid = threadIdx.x;
     const int m0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
-    const int tx = tid % 16, ty = tid / 16;
+    // 8 warps: warp w computes rows wm..wm+15 and columns wn..wn+31 of the tile.
+    const int warp = tid >> 5, lane = tid & 31;
+    const int wm = (warp & 3) * 16, wn = (warp >> 2) * 32;
+    const int g = lane >> 2, tq = lane & 3;  // MMA fragment coordinates
     float acc[4][4];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
@@ -85,29 +105,41 @@ __global__ void __launch_bounds__(256) gemm_kernel(const TA *__restrict__ A, int
             Bs[kk][nn] = v;
         }
         __syncthreads();
+        // Tensor cores: per 8-deep k step, the warp's 16 x 32 block of C as
+        // four m16n8k8 TF32 MMAs. A float32 operand is split into a TF32 high
+        // part and the TF32 rounding of its remainder, and the products
+        // hi*hi + hi*lo + lo*hi accumulate in float32, which keeps float32
+        // accuracy; a BF16 operand is exact in TF32 (no low part).
 #pragma unroll
-        for (int kk = 0; kk < 16; ++kk) {
-            float a[4], b[4];
+        for (int kk = 0; kk < 16; kk += 8) {
+            uint32_t ah[4], al[4];
+            {
+                const float av[4] = {As[kk + tq][wm + g], As[kk + tq][wm + g + 8], As[kk + tq + 4][wm + g],
+                                     As[kk + tq + 4][wm + g + 8]};
 #pragma unroll
-            for (int i = 0; i < 4; ++i) a[i] = As[kk][ty * 4 + i];
+                for (int i = 0; i < 4; ++i) split_tf32(av[i], ah[i], al[i]);
+            }
 #pragma unroll
-            for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx * 4 + j];
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+            for (int nt = 0; nt < 4; ++nt) {
+                const int nb = wn + nt * 8;
+                uint32_t bh[2], bl[2];
+                split_tf32(Bs[kk + tq][nb + g], bh[0], bl[0]);
+                split_tf32(Bs[kk + tq + 4][nb + g], bh[1], bl[1]);
+                mma_tf32(acc[nt], ah, bh);
+                mma_tf32(acc[nt], ah, bl);
+                mma_tf32(acc[nt], al, bh);
+            }
         }
         __syncthreads();
     }
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        const int gm = m0 + ty * 4 + i;
-        if (gm >= M) continue;
+    for (int nt = 0; nt < 4; ++nt) {
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int gn = n0 + tx * 4 + j;
-            if (gn >= N) continue;
-            float v = acc[i][j];
+        for (int h = 0; h < 4; ++h) {
+            const int gm = m0 + wm + g + (h >= 2 ? 8 : 0);
+            const int gn = n0 + wn + nt * 8 + 2 * tq + (h & 1);
+            if (gm >= M || gn >= N) continue;
+            float v = acc[nt][h];
             if (bias) v += bias[gn];
             if (relu) v = fmaxf(v, 0.f);
             float *c = C + (size_t) gm * ldc + gn;

@@ -66,6 +66,9 @@ constexpr int kHeadNbrs = kHeadWords - 1;
 #ifndef PANNS_FP8_MIXED
 #define PANNS_FP8_MIXED 1  // FP8 rows times a half-precision query by mixed-precision FMAs
 #endif
+#ifndef PANNS_HEAD_REGS
+#define PANNS_HEAD_REGS 0  // 1: head rows tested from registers, one candidate per chunk
+#endif
 #ifndef PANNS_SEARCH_MIN_BLOCKS
 #define PANNS_SEARCH_MIN_BLOCKS 6
 #endif
@@ -873,6 +876,41 @@ __device__ void search_one(const SearchArgs &a, const WarpMem &m, uint32_t q, ui
             // Lane j < gc also fetches candidate j's overflow offset (used if
             // its row is longer than the head row), in flight with the rows.
             const uint64_t my_off = (uint32_t) lane < gc ? __ldg(a.ovf_off + m.cand[c0 + lane]) : 0ull;
+#if PANNS_HEAD_REGS
+            // The head rows stay in registers: lane l holds word l of every
+            // candidate's row (word 0 the degree, words 1..31 neighbours), and
+            // the test-and-sets go by candidate, one row per chunk, so the
+            // neighbours keep their (candidate, slot) order.
+            uint32_t hv[kCandGroup], olds[kCandGroup];
+#pragma unroll
+            for (int j = 0; j < kCandGroup; ++j)
+                hv[j] = (uint32_t) j < gc ? __ldg(a.head + (size_t) m.cand[c0 + j] * kHeadWords + lane) : 0u;
+            uint32_t deg = 0, degsum = 0;
+#pragma unroll
+            for (int j = 0; j < kCandGroup; ++j) {
+                const uint32_t dj = __shfl_sync(kFull, hv[j], 0);  // 0 past the group
+                degsum += dj;
+                if (lane == j) deg = dj;
+                bool valid = lane >= 1 && (uint32_t) lane <= min(dj, (uint32_t) kHeadNbrs);
+                if (valid && hv[j] >= a.n) {
+                    atomicOr(a.error, ERR_BAD_ID);
+                    valid = false;
+                }
+                if (!valid) hv[j] = kFull;
+                olds[j] = visit_issue(vis, hv[j], valid);
+            }
+            n_edges += gc + degsum;
+            const bool any_long = __any_sync(kFull, deg > (uint32_t) kHeadNbrs);
+#pragma unroll
+            for (int j = 0; j < kCandGroup; ++j) {
+                if ((uint32_t) j >= gc) break;
+                const uint32_t id = hv[j];
+                const bool valid = id != kFull;
+                const bool fresh = valid && !(olds[j] & (1u << (id & 31)));
+                note_dirty(dirty, a.dirty_cap, dcount, valid && olds[j] == 0, id >> 5);
+                append_fresh<KIND, ORDER, CL, STORE>(a, m, nb, &sz, L, nk, n_dist, fresh, id, D, lane);
+            }
+#else
             {
                 uint32_t hv[kCandGroup];
 #pragma unroll
@@ -942,6 +980,7 @@ __device__ void search_one(const SearchArgs &a, const WarpMem &m, uint32_t q, ui
                 note_dirty(dirty, a.dirty_cap, dcount, valid && olds[ch] == 0, id >> 5);
                 append_fresh<KIND, ORDER, CL, STORE>(a, m, nb, &sz, L, nk, n_dist, fresh, id, D, lane);
             }
+#endif
             // Rows longer than the head row: the rest from the overflow lists
             // of all the group's long candidates, flattened in (candidate,
             // slot) order; per batch of kOvfChunks * 32 every load is issued

@@ -319,18 +319,31 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
                 __syncwarp();
                 if (lane == 0) mbar_arrive(t_empty + t);
-                float top_d = hd[r];
-                uint32_t top_i = hi[r];
+                // Screen distances, and a bit per column that beats the
+                // heap's top (the current C-th best) before this tile.
+                const float top_d = hd[r];
+                const uint32_t top_i = hi[r];
+                uint64_t beat = 0;
 #pragma unroll
                 for (int j = 0; j < 64; ++j) {
                     const float yj = __shfl_sync(0xffffffffu, j < 32 ? y0 : y1, j & 31);
-                    const uint32_t c = c0 + j;
                     const float sd = fmaf(-2.f, __uint_as_float(v[j]), yj);
-                    if (row < a.n && c < a.n && c != row && key_gt(top_d, top_i, sd, c)) {
-                        heap_replace_top(hd, hi, a.C, r, sd, c);
-                        top_d = hd[r];
-                        top_i = hi[r];
-                    }
+                    v[j] = __float_as_uint(sd);
+                    beat |= (uint64_t) key_gt(top_d, top_i, sd, c0 + j) << j;
+                }
+                if (row >= a.n) beat = 0;
+                const uint32_t self = row - c0;  // the row's own column, if in this tile
+                if (self < 64) beat &= ~(1ull << self);
+                if (c0 + 64 > a.n) beat &= a.n - c0 >= 64 ? ~0ull : ((1ull << (a.n - c0)) - 1);
+                // Insertions, in column order (each rechecked against the top).
+                while (beat) {
+                    const int j = __ffsll((long long) beat) - 1;
+                    beat &= beat - 1;
+                    float sd = 0.f;
+#pragma unroll
+                    for (int t = 0; t < 64; ++t)
+                        if (t == j) sd = __uint_as_float(v[t]);
+                    if (key_gt(hd[r], hi[r], sd, c0 + j)) heap_replace_top(hd, hi, a.C, r, sd, c0 + j);
                 }
             }
             if (*abort_flag) break;

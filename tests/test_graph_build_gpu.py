@@ -85,3 +85,17 @@ def test_gpu_graph_errors():
         build_nsg(x, R=6, knn_k=5)   # R <= k
     with pytest.raises(N.PannsError):
         build_nsg(np.zeros((300, 8), np.float32), R=4, knn_k=200)  # k <= 128
+
+
+def test_tcgen05_screen_many_row_blocks_per_cta():
+    """More row blocks than SMs (40,000 rows = 313 blocks of 128 on 148 SMs),
+    so each persistent CTA reloads its A operand and reuses its tensor memory
+    and heaps for several blocks: the graph equals the exact host build
+    (oracle/host_build.c, equal to the brute force)."""
+    from parallel_anns_b200 import datasets as ds
+    from parallel_anns_b200.graph import build_nsg
+    x = ds.gaussian_mixture(40000, 96, seed=12, means_seed=12)
+    g, knn = build_nsg(x, R=50, knn_k=64, with_knn=True, screen=3)
+    h, hknn = O.host_build_nsg(x, 64, 50)
+    assert np.array_equal(knn, hknn)
+    assert same_graph(g, h)

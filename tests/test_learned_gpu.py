@@ -71,7 +71,8 @@ def small():
     from parallel_anns_b200.searching import Index
     base = ds.gaussian_mixture(30000, 96, seed=501, means_seed=501)
     q = ds.gaussian_mixture(300, 96, seed=502, means_seed=501)
-    g = ds.build_nsg_graph(base, R=50, knn_k=64, device="cuda")
+    from parallel_anns_b200.graph import build_nsg
+    g = build_nsg(base, R=50, knn_k=64)  # the library's construction: the same graph in every process
     ix = Index(0)
     ix.set_base(base)
     ix.set_graph(g)
