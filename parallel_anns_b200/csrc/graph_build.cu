@@ -341,7 +341,9 @@ int panns_build_nsg_ex(int device, const float *base, uint32_t n, uint32_t d, ui
     if (screen > PANNS_SCREEN_TC) return set_error(PANNS_EINVAL, "panns_build_nsg: unknown screen");
     const uint32_t k = knn_k;
     const uint32_t C_tc = std::min(std::min(knn_k + 32u, (uint32_t) kMaxC), n - 1);
-    if (screen == PANNS_SCREEN_AUTO) screen = n < 100000 ? PANNS_SCREEN_FP32 : PANNS_SCREEN_TF32;
+    if (screen == PANNS_SCREEN_AUTO)
+        screen = n < 100000 ? PANNS_SCREEN_FP32
+                            : tc_screen_supported(n, d, C_tc) ? PANNS_SCREEN_TC : PANNS_SCREEN_TF32;
     if (screen == PANNS_SCREEN_TC && !tc_screen_supported(n, d, C_tc))
         return set_error(PANNS_EINVAL, "panns_build_nsg: the tcgen05 screen needs d a multiple of 32 up to 128 "
                                        "and n >= 128");

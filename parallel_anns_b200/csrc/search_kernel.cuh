@@ -67,7 +67,7 @@ constexpr int kHeadNbrs = kHeadWords - 1;
 #define PANNS_FP8_MIXED 1  // FP8 rows times a half-precision query by mixed-precision FMAs
 #endif
 #ifndef PANNS_HEAD_REGS
-#define PANNS_HEAD_REGS 0  // 1: head rows tested from registers, one candidate per chunk
+#define PANNS_HEAD_REGS 1  // head rows tested from registers, one candidate per chunk (0: staged and flattened)
 #endif
 #ifndef PANNS_SEARCH_MIN_BLOCKS
 #define PANNS_SEARCH_MIN_BLOCKS 6
