@@ -195,6 +195,7 @@ __device__ __forceinline__ void heap_replace_top(float *hd, uint32_t *hi, uint32
     hi[i * kTcM + r] = iv;
 }
 
+template <bool FUSED>
 __global__ void __launch_bounds__(kTcThreads, 1)
     tc_screen_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b,
                      TcArgs a) {
@@ -304,9 +305,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             for (uint32_t ct = 0; ct < col_tiles; ++ct, ++g) {
                 const uint32_t t = g & 1, tph = (g >> 1) & 1;
                 const uint32_t c0 = ct * kTcN;
-                // the 64 columns' norms, two per lane
-                const float y0 = c0 + lane < a.n ? __ldg(a.yn + c0 + lane) : 0.f;
-                const float y1 = c0 + 32 + lane < a.n ? __ldg(a.yn + c0 + 32 + lane) : 0.f;
+                // the 64 columns' norms, two per lane (already in the accumulators when FUSED)
+                const float y0 = !FUSED && c0 + lane < a.n ? __ldg(a.yn + c0 + lane) : 0.f;
+                const float y1 = !FUSED && c0 + 32 + lane < a.n ? __ldg(a.yn + c0 + 32 + lane) : 0.f;
                 bool ok = mbar_wait(t_full + t, tph);
                 ok = __all_sync(0xffffffffu, ok);
                 if (!ok) {
@@ -322,14 +323,26 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 // Screen distances, and a bit per column that beats the
                 // heap's top (the current C-th best) before this tile.
                 const float top_d = hd[r];
-                const uint32_t top_i = hi[r];
-                uint64_t beat = 0;
+                uint64_t beat;
+                if constexpr (FUSED) {
+                    // the accumulators hold ||y||^2 - 2 x.y; a distance equal to
+                    // the top's is decided by id in the insertion loop
+                    uint32_t lo = 0, hi32 = 0;
 #pragma unroll
-                for (int j = 0; j < 64; ++j) {
-                    const float yj = __shfl_sync(0xffffffffu, j < 32 ? y0 : y1, j & 31);
-                    const float sd = fmaf(-2.f, __uint_as_float(v[j]), yj);
-                    v[j] = __float_as_uint(sd);
-                    beat |= (uint64_t) key_gt(top_d, top_i, sd, c0 + j) << j;
+                    for (int j = 0; j < 32; ++j) lo |= (uint32_t) (__uint_as_float(v[j]) <= top_d) << j;
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) hi32 |= (uint32_t) (__uint_as_float(v[32 + j]) <= top_d) << j;
+                    beat = ((uint64_t) hi32 << 32) | lo;
+                } else {
+                    const uint32_t top_i = hi[r];
+                    beat = 0;
+#pragma unroll
+                    for (int j = 0; j < 64; ++j) {
+                        const float yj = __shfl_sync(0xffffffffu, j < 32 ? y0 : y1, j & 31);
+                        const float sd = fmaf(-2.f, __uint_as_float(v[j]), yj);
+                        v[j] = __float_as_uint(sd);
+                        beat |= (uint64_t) key_gt(top_d, top_i, sd, c0 + j) << j;
+                    }
                 }
                 if (row >= a.n) beat = 0;
                 const uint32_t self = row - c0;  // the row's own column, if in this tile
@@ -356,6 +369,31 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     if (warp == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcTmemCols));
+    }
+}
+
+// Rows with the norm folded into the contraction: xa = [x, 1, 1, 0...] and
+// xb = [-2x, hi, lo, 0...] (width w), hi = ||x||^2 cut to TF32 (exact in the
+// MMA), lo = the rest, so that xa_i . xb_j = ||x_j||^2 - 2 x_i . x_j.
+__global__ void augment_kernel(const float *__restrict__ x, const float *__restrict__ xn, uint32_t n, uint32_t d,
+                               uint32_t w, float *__restrict__ xa, float *__restrict__ xb) {
+    const uint64_t total = (uint64_t) n * w;
+    for (uint64_t t = blockIdx.x * (uint64_t) blockDim.x + threadIdx.x; t < total;
+         t += (uint64_t) gridDim.x * blockDim.x) {
+        const uint64_t r = t / w;
+        const uint32_t c = (uint32_t) (t % w);
+        float va = 0.f, vb = 0.f;
+        if (c < d) {
+            va = x[r * d + c];
+            vb = -2.f * va;
+        } else if (c == d || c == d + 1) {
+            va = 1.f;
+            const float y2 = xn[r];
+            const float hi = __uint_as_float(__float_as_uint(y2) & 0xffffe000u);
+            vb = c == d ? hi : y2 - hi;
+        }
+        xa[t] = va;
+        xb[t] = vb;
     }
 }
 
@@ -390,40 +428,66 @@ int tc_screen(const float *x, const float *xn, uint32_t n, uint32_t d, uint32_t 
               cudaStream_t s) {
     if (!tc_screen_supported(n, d, C)) return set_error(PANNS_EINVAL, "tc screen: unsupported shape");
     if (reinterpret_cast<uintptr_t>(x) % 16) return set_error(PANNS_EINVAL, "tc screen: base not 16-byte aligned");
-    const uint32_t slices = d / kTcSlice;
+    // The norm rides in an extra 32-wide slice when that still fits (d <= 96).
+    const bool fused = d + kTcSlice <= 128;
+    const uint32_t w = fused ? d + kTcSlice : d;
+    const uint32_t slices = w / kTcSlice;
     uint32_t stages = 4;
     while (stages > 2 && tc_layout(slices, stages, C).total + 1024 > 227u * 1024u) --stages;
     const TcSmem L = tc_layout(slices, stages, C);
     const size_t smem = L.total + 1024;
     if (smem > 227u * 1024u) return set_error(PANNS_EINVAL, "tc screen: C too large for shared memory");
-    CUtensorMap ma, mb;
-    int rc = make_map(&ma, x, n, d, kTcM);
-    if (!rc) rc = make_map(&mb, x, n, d, kTcN);
-    if (rc) return rc;
+    float *xa = nullptr, *xb = nullptr;
     uint32_t *err = nullptr;
     cudaError_t e = cudaMallocAsync(&err, 4, s);
-    if (e != cudaSuccess) return set_error(PANNS_ECUDA, std::string("tc screen: ") + cudaGetErrorString(e));
+    if (e == cudaSuccess && fused) e = cudaMallocAsync(&xa, (size_t) n * w * 4, s);
+    if (e == cudaSuccess && fused) e = cudaMallocAsync(&xb, (size_t) n * w * 4, s);
+    if (e != cudaSuccess) {
+        cudaFreeAsync(err, s);
+        if (xa) cudaFreeAsync(xa, s);
+        return set_error(PANNS_ECUDA, std::string("tc screen: ") + cudaGetErrorString(e));
+    }
     cudaMemsetAsync(err, 0, 4, s);
+    if (fused) {
+        const uint64_t total = (uint64_t) n * w;
+        const int blocks = (int) std::min<uint64_t>((total + 255) / 256, (uint64_t) num_sms * 32);
+        augment_kernel<<<blocks, 256, 0, s>>>(x, xn, n, d, w, xa, xb);
+    }
+    CUtensorMap ma, mb;
+    int rc = make_map(&ma, fused ? xa : x, n, w, kTcM);
+    if (!rc) rc = make_map(&mb, fused ? xb : x, n, w, kTcN);
+    if (rc) {
+        cudaFreeAsync(err, s);
+        if (xa) cudaFreeAsync(xa, s);
+        if (xb) cudaFreeAsync(xb, s);
+        return rc;
+    }
     TcArgs a;
     a.yn = xn;
     a.n = n;
-    a.d = d;
+    a.d = w;
     a.C = C;
     a.slices = slices;
     a.stages = stages;
     a.cand = cand;
     a.error = err;
-    e = cudaFuncSetAttribute(tc_screen_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+    const void *kern = fused ? (const void *) tc_screen_kernel<true> : (const void *) tc_screen_kernel<false>;
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
     if (e == cudaSuccess) {
         const uint32_t row_blocks = (n + kTcM - 1) / kTcM;
         const uint32_t grid = std::min<uint32_t>(row_blocks, (uint32_t) num_sms);
-        tc_screen_kernel<<<grid, kTcThreads, smem, s>>>(ma, mb, a);
+        if (fused) tc_screen_kernel<true><<<grid, kTcThreads, smem, s>>>(ma, mb, a);
+        else tc_screen_kernel<false><<<grid, kTcThreads, smem, s>>>(ma, mb, a);
         e = cudaGetLastError();
     }
     uint32_t herr = 0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     cudaFreeAsync(err, s);
+    if (xa) cudaFreeAsync(xa, s);
+    if (xb) cudaFreeAsync(xb, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return set_error(PANNS_ECUDA, std::string("tc screen: ") + cudaGetErrorString(e));
     if (herr) return set_error(PANNS_EDEVICE, "tc screen: an mbarrier wait expired");
     return PANNS_OK;
