@@ -66,6 +66,9 @@ constexpr int kHeadNbrs = kHeadWords - 1;
 #ifndef PANNS_FP8_MIXED
 #define PANNS_FP8_MIXED 1  // FP8 rows times a half-precision query by mixed-precision FMAs
 #endif
+#ifndef PANNS_RERANK_WIDE
+#define PANNS_RERANK_WIDE 0  // 1: the final exact re-rank with 16 rows in flight per warp pass
+#endif
 #ifndef PANNS_SORT32_BITONIC
 #define PANNS_SORT32_BITONIC 0  // 1: up to 32 survivors sorted by a register bitonic network
 #endif
@@ -1080,7 +1083,11 @@ __device__ void search_one(const SearchArgs &a, const WarpMem &m, uint32_t q, ui
         // order); the K best by (distance, original id) go out.
         Dist<KIND, CL, STORE_FP32> E;
         E.load(a, q, lane);
+#if PANNS_RERANK_WIDE
+        distances_wide<KIND, CL>(a, E.qv, m.qi, m.qd, sz, lane);  // 16 rows in flight per pass
+#else
         E.distances(a, m.qi, m.qd, sz, lane);
+#endif
         rerank_output(m.qd, m.qi, sz, a.K, a.orig, a.out_ids + (size_t) q * a.K, lane);
     } else {
         // Results (original ids).
