@@ -66,12 +66,6 @@ constexpr int kHeadNbrs = kHeadWords - 1;
 #ifndef PANNS_FP8_MIXED
 #define PANNS_FP8_MIXED 1  // FP8 rows times a half-precision query by mixed-precision FMAs
 #endif
-#ifndef PANNS_RERANK_WIDE
-#define PANNS_RERANK_WIDE 0  // 1: the final exact re-rank with 16 rows in flight per warp pass
-#endif
-#ifndef PANNS_SORT32_BITONIC
-#define PANNS_SORT32_BITONIC 0  // 1: up to 32 survivors sorted by a register bitonic network
-#endif
 #ifndef PANNS_HEAD_REGS
 #define PANNS_HEAD_REGS 1  // head rows tested from registers, one candidate per chunk (0: staged and flattened)
 #endif
@@ -300,38 +294,6 @@ __device__ void warp_sort(float *bd, uint32_t *bi, uint32_t *bk, uint32_t cnt,
                           const uint32_t *orig, int lane) {
     (void) orig;
     if (cnt <= 1) return;
-#if PANNS_SORT32_BITONIC
-    if (cnt <= 32) {
-        // one element per lane, a bitonic network by shuffles
-        float d = (uint32_t) lane < cnt ? bd[lane] : __int_as_float(0x7f800000);
-        uint32_t k = (uint32_t) lane < cnt ? bk[lane] : kFull;
-        uint32_t v = (uint32_t) lane < cnt ? bi[lane] : 0u;
-#pragma unroll
-        for (int kk = 2; kk <= 32; kk <<= 1) {
-#pragma unroll
-            for (int j = kk >> 1; j > 0; j >>= 1) {
-                const float od = __shfl_xor_sync(kFull, d, j);
-                const uint32_t ok = __shfl_xor_sync(kFull, k, j);
-                const uint32_t ov = __shfl_xor_sync(kFull, v, j);
-                const bool up = (lane & kk) == 0, lower = (lane & j) == 0;
-                const bool take = (lower == up) ? plain_less(od, ok, d, k) : plain_less(d, k, od, ok);
-                if (take) {
-                    d = od;
-                    k = ok;
-                    v = ov;
-                }
-            }
-        }
-        __syncwarp();
-        if ((uint32_t) lane < cnt) {
-            bd[lane] = d;
-            bk[lane] = k;
-            bi[lane] = v;
-        }
-        __syncwarp();
-        return;
-    }
-#endif
     if (cnt <= 64) {
         const uint32_t j0 = lane, j1 = lane + 32;
         const bool h0 = j0 < cnt, h1 = j1 < cnt;
@@ -1083,11 +1045,7 @@ __device__ void search_one(const SearchArgs &a, const WarpMem &m, uint32_t q, ui
         // order); the K best by (distance, original id) go out.
         Dist<KIND, CL, STORE_FP32> E;
         E.load(a, q, lane);
-#if PANNS_RERANK_WIDE
-        distances_wide<KIND, CL>(a, E.qv, m.qi, m.qd, sz, lane);  // 16 rows in flight per pass
-#else
         E.distances(a, m.qi, m.qd, sz, lane);
-#endif
         rerank_output(m.qd, m.qi, sz, a.K, a.orig, a.out_ids + (size_t) q * a.K, lane);
     } else {
         // Results (original ids).
