@@ -57,9 +57,20 @@ def build(force: bool = False, verbose: bool = False, extra=None, out: str | Non
     os.makedirs(objdir, exist_ok=True)
     procs = []
     objs = []
+    # An object is reused when it is newer than its source and every shared
+    # header, and was built with the same flags (recorded beside it).
+    headers = [p for p in DEPS if p not in SOURCES and os.path.exists(p)]
+    newest_header = max((os.path.getmtime(p) for p in headers), default=0.0)
+    flags_key = " ".join(NVCC_FLAGS + (extra or []))
     for src in SOURCES:
         obj = os.path.join(objdir, os.path.basename(src) + ".o")
         objs.append(obj)
+        stamp = obj + ".flags"
+        if (os.path.exists(obj) and os.path.exists(stamp) and open(stamp).read() == flags_key
+                and os.path.getmtime(obj) > max(os.path.getmtime(src), newest_header)):
+            continue
+        with open(stamp, "w") as f:
+            f.write(flags_key)
         cmd = [nvcc()] + NVCC_FLAGS + (extra or []) + ["-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)

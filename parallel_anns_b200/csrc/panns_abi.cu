@@ -893,8 +893,12 @@ static int launch_search(panns_index *h, const panns_search_params *p, float *d_
         if (changed) {
             h->mlp.logits = h->mlp_logits.p;
             h->mlp.record = h->mlp_record.p;
+            // On the launch stream (a plain cudaMemcpy from pageable memory may
+            // return before its DMA lands, and the handle's streams are not
+            // ordered after the legacy stream), complete before h->mlp changes.
             CU(cudaStreamSynchronize(stream));
-            CU(cudaMemcpy(h->mlp_dev.p, &h->mlp, sizeof(MlpDev), cudaMemcpyHostToDevice));
+            CU(cudaMemcpyAsync(h->mlp_dev.p, &h->mlp, sizeof(MlpDev), cudaMemcpyHostToDevice, stream));
+            CU(cudaStreamSynchronize(stream));
         }
         h->mlp_last_nq = nq;
     }
@@ -1016,7 +1020,8 @@ static int stage_init(panns_index *h, const panns_search_params *p, const uint32
     }
     if (!efanna && !init_ids) {
         CU(h->init_def.ensure(L));
-        CU(cudaMemcpy(h->init_def.p, dev.data(), (size_t) L * 4, cudaMemcpyHostToDevice));
+        // Ordered on the launch stream (the source is staged before the call returns).
+        CU(cudaMemcpyAsync(h->init_def.p, dev.data(), (size_t) L * 4, cudaMemcpyHostToDevice, stream));
         h->init_def_L = L;
         d_init = h->init_def.p;
         return PANNS_OK;
@@ -1508,10 +1513,15 @@ extern "C" int panns_set_learned(panns_index *h, const float *params, uint32_t R
         rep[i] = h->inv[rep_ids[i]];
     }
     CU(cudaSetDevice(h->device));
+    // Searches still in flight (on any stream) read the network being replaced.
+    CU(cudaDeviceSynchronize());
     const uint64_t P = panns_mlp_param_count(h->d, R);
     DevBuf<float> dp;
     CU(dp.ensure(P));
-    CU(cudaMemcpy(dp.p, params, P * 4, cudaMemcpyHostToDevice));
+    // Every copy goes on the handle's stream, which the packing kernel and the
+    // searches use: a plain cudaMemcpy from pageable memory may return before
+    // its DMA lands, and that stream (non-blocking) is not ordered after it.
+    CU(cudaMemcpyAsync(dp.p, params, P * 4, cudaMemcpyHostToDevice, h->stream));
     CU(h->mlp_w.ensure((size_t) kMlpH * (h->d + kMlpH + R)));
     CU(h->mlp_f.ensure(3u * kMlpH + R + 1));
     CU(h->mlp_rep.ensure(R));
@@ -1550,7 +1560,8 @@ extern "C" int panns_set_learned(panns_index *h, const float *params, uint32_t R
         m.logits = nullptr;
     }
     h->mlp = m;
-    CU(cudaMemcpy(h->mlp_dev.p, &h->mlp, sizeof(MlpDev), cudaMemcpyHostToDevice));
+    CU(cudaMemcpyAsync(h->mlp_dev.p, &h->mlp, sizeof(MlpDev), cudaMemcpyHostToDevice, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
     h->has_mlp = true;
     return PANNS_OK;
 }
