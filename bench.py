@@ -422,7 +422,7 @@ def bench_ours(args):
         outb = torch.empty((B, K), dtype=torch.int32, device="cuda")
         best_b, tried = None, {}
         # the head's own configuration, then the head's storage, L and M
-        # without the learned prologue, with 1, 2 and 4 warps per query
+        # without the learned network, with 1, 2 and 4 warps per query
         options = [(head.warps_per_query, ixh, dict(kw, flags=kw["flags"] | N.FLAG_CUDA_GRAPH))]
         for wq in (1, 2, 4, 8):
             if wq == head.warps_per_query and head.learned is None:

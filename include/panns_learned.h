@@ -29,8 +29,10 @@
 extern "C" {
 #endif
 
-/* Searches with this flag run the attached network in the kernel prologue
- * (NSG_SEQ, TOP_M and PSS_V5 at T = 1; any storage). */
+/* Searches with this flag run the attached network over the whole batch just
+ * before the search kernel (tensor-core GEMMs), and each query's search
+ * starts from that query's decision (NSG_SEQ, TOP_M and PSS_V5 at T = 1;
+ * any storage). */
 #define PANNS_FLAG_LEARNED 2u
 
 /* Number of float32 parameters of the network for input width d and R classes. */

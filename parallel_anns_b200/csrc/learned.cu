@@ -2,10 +2,11 @@
 // L-budget network's training (forward, backward, Adam) on the GPU.
 //
 // Training shapes are small (batch x {d, 256, R + 1}), so one generic tiled
-// float32 GEMM serves every product of the forward and backward passes,
-// reading the weight matrices as BF16 (the precision the search-kernel
-// prologue uses). Everything is deterministic: fixed reduction orders, no
-// floating-point atomics, a seeded sample order.
+// GEMM (tensor cores, float32 accuracy) serves every product of the forward
+// and backward passes, reading the weight matrices as BF16 (the precision
+// inference uses: the same GEMMs run the batched forward pass of mlp_decide).
+// Everything is deterministic: fixed reduction orders, no floating-point
+// atomics, a seeded sample order.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -619,6 +620,127 @@ int mlp_pack_inference(const float *params_dev, uint32_t d, uint32_t R, void *wb
     pack_kernel<<<256, 256, 0, s>>>(params_dev, d, R, reinterpret_cast<__nv_bfloat16 *>(wbf), fb);
     LCU(cudaGetLastError());
     return PANNS_OK;
+}
+
+namespace {
+// X[q][i] = query q's element i, from the chain-major rows (width dpad).
+__global__ void rows_from_chain_major_kernel(const float *__restrict__ q_cm, uint32_t dpad, uint32_t d, uint32_t nq,
+                                             float *__restrict__ X) {
+    const size_t total = (size_t) nq * d;
+    for (size_t t = blockIdx.x * (size_t) blockDim.x + threadIdx.x; t < total; t += (size_t) gridDim.x * blockDim.x) {
+        const size_t q = t / d;
+        const uint32_t i = (uint32_t) (t - q * d);
+        X[t] = q_cm[q * dpad + chain_major_index(d, i)];
+    }
+}
+
+// One warp per query: the decision from its logits Z[q] (R) and its second
+// hidden layer H2[q] (256). Lane t owns logits t, t + 32, ... (R / 32 <= 32
+// of them in registers) and hidden units 8t..8t+7.
+__global__ void __launch_bounds__(256) decide_kernel(MlpDev m, const float *__restrict__ H2,
+                                                     const float *__restrict__ Z, uint32_t nq, uint32_t L,
+                                                     const uint32_t *__restrict__ Lq_in, uint32_t K,
+                                                     uint32_t *__restrict__ record) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t q = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (q >= nq) return;
+    const uint32_t R = m.R, nc = R / 32;
+    // L-budget regressor.
+    const float *h = H2 + (size_t) q * kMlpH + lane * 8;
+    float r = 0.f;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) r = fmaf(m.wl[lane * 8 + j], h[j], r);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+    r += m.bl;
+    // Logits and the largest softmax probability.
+    const float *z = Z + (size_t) q * R;
+    float v[kMlpMaxR / 32];
+    float mx = PANNS_NEG_INF;
+#pragma unroll
+    for (int c = 0; c < kMlpMaxR / 32; ++c) {
+        v[c] = (uint32_t) c < nc ? z[c * 32 + lane] : PANNS_NEG_INF;
+        mx = fmaxf(mx, v[c]);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    float se = 0.f;
+#pragma unroll
+    for (int c = 0; c < kMlpMaxR / 32; ++c)
+        if ((uint32_t) c < nc) se += expf(v[c] - mx);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) se += __shfl_xor_sync(0xffffffffu, se, o);
+    const float conf = 1.f / se;  // softmax probability of the largest logit
+    const bool fallback = !(conf >= m.min_conf);
+    const uint32_t Lc = Lq_in ? Lq_in[q] : L;
+    uint32_t Lq = Lc;
+    if (!fallback && m.use_L) {
+        const float x = m.L_scale * expf(m.L_exp * r);
+        const uint32_t lo = max(K, min(m.L_min, Lc));
+        if (x < (float) Lc) Lq = max(lo, (uint32_t) ceilf(fmaxf(x, 0.f)));
+    }
+    uint32_t *rec = record + (size_t) q * kMlpRecWords;
+    uint32_t E = 0;
+    if (!fallback && m.use_entry) {
+        // The E largest logits, one warp argmax each (ties to the lower index).
+        const uint32_t want = min(min(m.E, (uint32_t) kMlpMaxE), Lq);
+        for (; E < want; ++E) {
+            float best = PANNS_NEG_INF;
+            uint32_t bi = 0xffffffffu;
+#pragma unroll
+            for (int c = 0; c < kMlpMaxR / 32; ++c)
+                if (v[c] > best) {
+                    best = v[c];
+                    bi = c * 32 + lane;
+                }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const float b2 = __shfl_xor_sync(0xffffffffu, best, o);
+                const uint32_t i2 = __shfl_xor_sync(0xffffffffu, bi, o);
+                if (b2 > best || (b2 == best && i2 < bi)) {
+                    best = b2;
+                    bi = i2;
+                }
+            }
+            if (bi >= R) break;  // only -inf or NaN left
+            if (lane == 0) rec[2 + E] = __ldg(m.rep + bi);
+            if (lane == (int) (bi & 31)) {
+#pragma unroll
+                for (int c = 0; c < kMlpMaxR / 32; ++c)
+                    if ((uint32_t) c == (bi >> 5)) v[c] = PANNS_NEG_INF;
+            }
+        }
+    }
+    if (lane == 0) {
+        rec[0] = Lq | (fallback ? 0x80000000u : 0u);
+        rec[1] = E;
+    }
+}
+}  // namespace
+
+cudaError_t mlp_decide(const MlpDev &m, const float *q_cm, uint32_t dpad, uint32_t nq, uint32_t L, const uint32_t *Lq,
+                       uint32_t K, const MlpScratch &w, uint32_t *record, cudaStream_t s) {
+    const int H = kMlpH, d = (int) m.d, R = (int) m.R;
+    cudaError_t e = cudaSuccess;
+    for (uint32_t r0 = 0; r0 < nq && e == cudaSuccess; r0 += w.rows) {
+        const uint32_t rows = std::min(w.rows, nq - r0);
+        const size_t total = (size_t) rows * m.d;
+        rows_from_chain_major_kernel<<<(unsigned) std::min<size_t>((total + 255) / 256, 4096), 256, 0, s>>>(
+            q_cm + (size_t) r0 * dpad, dpad, m.d, rows, w.X);
+        e = cudaGetLastError();
+        if (e == cudaSuccess)
+            e = gemm<float, __nv_bfloat16, false, false>(w.X, d, m.w1, H, w.H1, H, (int) rows, H, d, m.b1, 1, s);
+        if (e == cudaSuccess)
+            e = gemm<float, __nv_bfloat16, false, false>(w.H1, H, m.w2, H, w.H2, H, (int) rows, H, H, m.b2, 1, s);
+        if (e == cudaSuccess)
+            e = gemm<float, __nv_bfloat16, false, false>(w.H2, H, m.w3, R, w.Z, R, (int) rows, R, H, m.b3, 0, s);
+        if (e == cudaSuccess) {
+            decide_kernel<<<(rows + 7) / 8, 256, 0, s>>>(m, w.H2, w.Z, rows, L, Lq ? Lq + r0 : nullptr, K,
+                                                         record + (size_t) r0 * kMlpRecWords);
+            e = cudaGetLastError();
+        }
+    }
+    return e;
 }
 
 }  // namespace panns

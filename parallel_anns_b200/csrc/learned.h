@@ -7,6 +7,8 @@
 
 #include <string>
 
+#include "mlp_infer.cuh"
+
 namespace panns {
 
 // Records `msg` as the calling thread's last error (panns_last_error) and
@@ -29,10 +31,27 @@ int nearest_center(const float *rows, uint32_t n, uint32_t d, const uint32_t *ce
                    uint32_t *cell, cudaStream_t stream);
 
 // Packs the float32 training parameters (layout of panns_mlp_param_count)
-// into the inference layout read by mlp_prologue: BF16 w1 (d x 256),
+// into the inference layout read by mlp_decide: BF16 w1 (d x 256),
 // w2 (256 x 256), w3 (256 x R) into `wbf` (device, 256 (d + 256 + R)
 // elements) and float32 b1, b2, b3, wl, bl into `fb` (device, 256 * 3 + R + 1).
 int mlp_pack_inference(const float *params_dev, uint32_t d, uint32_t R, void *wbf, float *fb,
                        cudaStream_t stream);
+
+// Device scratch of mlp_decide for a chunk of `rows` queries: X (rows x d),
+// H1 and H2 (rows x 256), Z (rows x R).
+struct MlpScratch {
+    float *X, *H1, *H2, *Z;
+    uint32_t rows;
+};
+
+// Batched inference of the network `m` (device pointers) for nq queries,
+// chain-major rows of width dpad at q_cm (device): per chunk of scratch.rows
+// queries, the three layers as tensor-core GEMMs, then each query's decision
+// record (kMlpRecWords words: L_q | fallback << 31, E, E entry vertices as
+// device ids) into `record`. The call's queue length is L, or Lq[q] when Lq
+// (device) is given. Only enqueues on `stream` (graph-capturable); returns the
+// first launch error.
+cudaError_t mlp_decide(const MlpDev &m, const float *q_cm, uint32_t dpad, uint32_t nq, uint32_t L, const uint32_t *Lq,
+               uint32_t K, const MlpScratch &scratch, uint32_t *record, cudaStream_t stream);
 
 }  // namespace panns

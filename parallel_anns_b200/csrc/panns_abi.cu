@@ -192,14 +192,14 @@ struct panns_index {
     std::vector<uint8_t> gkey;
     // Learned entry / L-budget network (PANNS_FLAG_LEARNED).
     bool has_mlp = false;
-    MlpDev mlp{};                  // host copy of the device struct
-    DevBuf<uint8_t> mlp_dev;       // the struct on the device
+    MlpDev mlp{};                  // the network (device pointers) and decision rule
     DevBuf<uint16_t> mlp_w;        // BF16 weights, inference layout
     DevBuf<float> mlp_f;           // biases and regressor
     DevBuf<uint32_t> mlp_rep;      // representatives (device ids)
-    DevBuf<float> mlp_logits;      // slots x R
-    DevBuf<uint32_t> mlp_record;   // per query of the last call
-    uint32_t mlp_slots = 0, mlp_rec_cap = 0, mlp_last_nq = 0;
+    DevBuf<float> mlp_scratch;     // batched inference: X, H1, H2, Z of one chunk of queries
+    uint32_t mlp_chunk = 0;        // queries per chunk the scratch holds
+    DevBuf<uint32_t> mlp_record;   // per-query decisions of the last call
+    uint32_t mlp_rec_cap = 0, mlp_last_nq = 0;
 };
 
 extern "C" {
@@ -701,6 +701,13 @@ struct LaunchDesc {
     const float *rows;      // row-major queries to lay out into rows_cm (or null)
     float *rows_cm;
     uint32_t rows_n, d, dpad;
+    // Learned decisions computed before the search (mlp_decide), or mlp null.
+    const MlpDev *mlp;
+    const float *mlp_q;     // chain-major queries
+    uint32_t mlp_nq, mlp_L, mlp_K;
+    const uint32_t *mlp_Lq;
+    MlpScratch mlp_scratch;
+    uint32_t *mlp_record;
 };
 
 static cudaError_t enqueue_plain(const LaunchDesc &l, int num_sms, cudaStream_t s) {
@@ -713,6 +720,8 @@ static cudaError_t enqueue_plain(const LaunchDesc &l, int num_sms, cudaStream_t 
                                                              (int) l.dpad, nullptr);
         e = cudaGetLastError();
     }
+    if (e == cudaSuccess && l.mlp)
+        e = mlp_decide(*l.mlp, l.mlp_q, l.dpad, l.mlp_nq, l.mlp_L, l.mlp_Lq, l.mlp_K, l.mlp_scratch, l.mlp_record, s);
     if (e == cudaSuccess) {
         void *argv[] = {const_cast<void *>(l.args)};
         e = cudaLaunchKernel(l.kern, dim3(l.blocks), dim3(l.threads), argv, l.smem, s);
@@ -734,8 +743,14 @@ static int enqueue_launch(panns_index *h, const LaunchDesc &l, cudaStream_t s, b
     const uint64_t f[] = {(uint64_t) (uintptr_t) l.kern, l.blocks, l.threads, l.smem,
                           (uint64_t) (uintptr_t) l.counter, (uint64_t) (uintptr_t) l.error,
                           (uint64_t) (uintptr_t) l.rows, (uint64_t) (uintptr_t) l.rows_cm,
-                          l.rows_n, l.d, l.dpad};
+                          l.rows_n, l.d, l.dpad,
+                          (uint64_t) (uintptr_t) l.mlp, (uint64_t) (uintptr_t) l.mlp_q, l.mlp_nq, l.mlp_L, l.mlp_K,
+                          (uint64_t) (uintptr_t) l.mlp_Lq, (uint64_t) (uintptr_t) l.mlp_scratch.X,
+                          (uint64_t) (uintptr_t) l.mlp_scratch.H1, (uint64_t) (uintptr_t) l.mlp_scratch.H2,
+                          (uint64_t) (uintptr_t) l.mlp_scratch.Z, l.mlp_scratch.rows,
+                          (uint64_t) (uintptr_t) l.mlp_record};
     put(f, sizeof(f));
+    if (l.mlp) put(l.mlp, sizeof(MlpDev));  // value-initialised, so padding compares equal
     put(l.args, l.args_size);  // zero-filled structs, so padding compares equal
     if (!h->gexec || key != h->gkey) {
         cudaGraph_t g = nullptr;
@@ -877,34 +892,24 @@ static int launch_search(panns_index *h, const panns_search_params *p, float *d_
     CU(h->error.ensure(1));
     const bool learned = (p->flags & PANNS_FLAG_LEARNED) != 0;
     if (learned) {
-        // Scratch of the prologue sized for this launch; the device struct is
-        // re-uploaded (synchronously, outside any capture) when it changes.
-        bool changed = false;
-        if (h->mlp_slots < nslots) {
-            CU(h->mlp_logits.ensure((size_t) nslots * h->mlp.R));
-            h->mlp_slots = nslots;
-            changed = true;
+        // Scratch of the batched inference (chunks of up to 16,384 queries)
+        // and the per-query decision records, sized before any capture.
+        const uint32_t chunk = std::min<uint32_t>(nq, 16384);
+        if (h->mlp_chunk < chunk || h->mlp_scratch.n < (size_t) h->mlp_chunk * (h->d + 2u * kMlpH + h->mlp.R)) {
+            const uint32_t c = std::max(chunk, h->mlp_chunk);
+            CU(h->mlp_scratch.ensure((size_t) c * (h->d + 2u * kMlpH + h->mlp.R)));
+            h->mlp_chunk = c;
         }
         if (h->mlp_rec_cap < nq) {
             CU(h->mlp_record.ensure((size_t) nq * kMlpRecWords));
             h->mlp_rec_cap = nq;
-            changed = true;
-        }
-        if (changed) {
-            h->mlp.logits = h->mlp_logits.p;
-            h->mlp.record = h->mlp_record.p;
-            // On the launch stream (a plain cudaMemcpy from pageable memory may
-            // return before its DMA lands, and the handle's streams are not
-            // ordered after the legacy stream), complete before h->mlp changes.
-            CU(cudaStreamSynchronize(stream));
-            CU(cudaMemcpyAsync(h->mlp_dev.p, &h->mlp, sizeof(MlpDev), cudaMemcpyHostToDevice, stream));
-            CU(cudaStreamSynchronize(stream));
         }
         h->mlp_last_nq = nq;
     }
     SearchArgs a;
     memset(&a, 0, sizeof(a));
-    a.mlp = learned ? reinterpret_cast<const MlpDev *>(h->mlp_dev.p) : nullptr;
+    a.decisions = learned ? h->mlp_record.p : nullptr;
+    a.dec_L_init = h->mlp.L_init;
     a.vec = reinterpret_cast<const float4 *>(h->vec.p);
     a.norms = h->norms.p;
     a.head = h->head.p;
@@ -958,6 +963,19 @@ static int launch_search(panns_index *h, const panns_search_params *p, float *d_
     l.rows_n = nq;
     l.d = h->d;
     l.dpad = h->dpad;
+    if (learned) {
+        l.mlp = &h->mlp;
+        l.mlp_q = d_queries_cm;
+        l.mlp_nq = nq;
+        l.mlp_L = p->L;
+        l.mlp_K = p->K;
+        l.mlp_Lq = d_lq;
+        float *sp = h->mlp_scratch.p;
+        const size_t c = h->mlp_chunk;
+        l.mlp_scratch = MlpScratch{sp, sp + c * h->d, sp + c * (h->d + kMlpH), sp + c * (h->d + 2u * kMlpH),
+                                   h->mlp_chunk};
+        l.mlp_record = h->mlp_record.p;
+    }
     if (time_it) CU(cudaEventRecord(h->ev0, stream));
     int rc = enqueue_launch(h, l, stream, (p->flags & PANNS_FLAG_CUDA_GRAPH) != 0);
     if (rc) return rc;
@@ -1525,7 +1543,6 @@ extern "C" int panns_set_learned(panns_index *h, const float *params, uint32_t R
     CU(h->mlp_w.ensure((size_t) kMlpH * (h->d + kMlpH + R)));
     CU(h->mlp_f.ensure(3u * kMlpH + R + 1));
     CU(h->mlp_rep.ensure(R));
-    CU(h->mlp_dev.ensure(sizeof(MlpDev)));
     rc = panns::mlp_pack_inference(dp.p, h->d, R, h->mlp_w.p, h->mlp_f.p, h->stream);
     if (rc) return rc;
     CU(cudaMemcpyAsync(h->mlp_rep.p, rep.data(), R * 4ull, cudaMemcpyHostToDevice, h->stream));
@@ -1553,15 +1570,8 @@ extern "C" int panns_set_learned(panns_index *h, const float *params, uint32_t R
     m.min_conf = lp->min_conf;
     m.L_scale = lp->L_scale;
     m.L_exp = lp->L_exp;
-    m.logits = h->mlp_logits.p;
-    m.record = h->mlp_record.p;
-    if (h->mlp_slots && h->mlp_logits.n < (size_t) h->mlp_slots * R) {  // R grew: re-size at the next launch
-        h->mlp_slots = 0;
-        m.logits = nullptr;
-    }
+    if (h->mlp.R != R) h->mlp_chunk = 0;  // the inference scratch is re-sized at the next launch
     h->mlp = m;
-    CU(cudaMemcpyAsync(h->mlp_dev.p, &h->mlp, sizeof(MlpDev), cudaMemcpyHostToDevice, h->stream));
-    CU(cudaStreamSynchronize(h->stream));
     h->has_mlp = true;
     return PANNS_OK;
 }

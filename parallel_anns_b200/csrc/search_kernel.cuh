@@ -38,7 +38,7 @@
 //         read per expansion); ovf_off/ovf: the rest of longer rows (CSR).
 //
 // Per warp (shared memory): the queue (L x (dist f32, id u32 with bit 31 =
-// checked)), a buffer of fresh candidates, staged head rows. Per warp slot in
+// checked)), a buffer of fresh candidates, the picked candidates. Per warp slot in
 // global memory: a visited bitset of n bits plus the list of its words that
 // went from zero to non-zero, so only those are cleared after the query.
 #pragma once
@@ -66,17 +66,16 @@ constexpr int kHeadNbrs = kHeadWords - 1;
 #ifndef PANNS_FP8_MIXED
 #define PANNS_FP8_MIXED 1  // FP8 rows times a half-precision query by mixed-precision FMAs
 #endif
-#ifndef PANNS_HEAD_REGS
-#define PANNS_HEAD_REGS 1  // head rows tested from registers, one candidate per chunk (0: staged and flattened)
-#endif
 #ifndef PANNS_SEARCH_MIN_BLOCKS
 #define PANNS_SEARCH_MIN_BLOCKS 6
 #endif
 constexpr int kBuf = PANNS_KBUF;  // fresh-candidate buffer per warp
 // warp_sort pads a chunk to the next power of two >= its size inside the buffer.
 static_assert(kBuf >= 64 && (kBuf & (kBuf - 1)) == 0, "kBuf must be a power of two >= 64");
-constexpr int kCandGroup = 8;    // candidates whose head rows are staged at once
+constexpr int kCandGroup = 8;    // candidates whose head rows are loaded at once
 constexpr int kGroupChunks = (kCandGroup * kHeadNbrs + 31) / 32;
+// A group's head-row neighbours go into the fresh buffer without a flush in between.
+static_assert(kCandGroup * kHeadNbrs <= kBuf, "kBuf must hold a group's head-row neighbours");
 constexpr int kOvfChunks = 2;    // overflow neighbours per batch of loads: kOvfChunks * 32
 constexpr int kMaxM = 64;
 
@@ -117,7 +116,8 @@ struct SearchArgs {
     const float *scales;      // FP8: per-dimension scale (dpad)
     uint32_t d;               // dimension
     const uint32_t *Lq;       // per-query queue length (K <= Lq[q] <= L), or null: L for all
-    const MlpDev *mlp;        // entry / L-budget network run in the prologue, or null
+    const uint32_t *decisions;  // per-query records of the entry / L-budget network (mlp_decide), or null
+    uint32_t dec_L_init;      // plain init ids kept after learned entries
     uint32_t block_round;     // search_block_kernel: candidates per warp and merge round
 };
 
@@ -125,9 +125,7 @@ struct SearchArgs {
 __host__ __device__ inline uint32_t warp_smem_bytes(uint32_t queue_cap) {
     return queue_cap * 8u                 // queue dist + id
            + kBuf * 12u                   // buffer dist + id + key
-           + kCandGroup * kHeadWords * 4u // staged head rows
-           + kMaxM * 4u                   // picked candidate ids
-           + 64u * 4u;                    // prefix sums / scratch
+           + kMaxM * 4u;                  // picked candidate ids / learned entries
 }
 
 struct WarpMem {
@@ -136,9 +134,7 @@ struct WarpMem {
     float *bd;
     uint32_t *bi;
     uint32_t *bk;
-    uint32_t *hrow;
     uint32_t *cand;
-    uint32_t *pre;
 };
 
 static __device__ __forceinline__ WarpMem carve(uint8_t *base, uint32_t queue_cap) {
@@ -148,9 +144,7 @@ static __device__ __forceinline__ WarpMem carve(uint8_t *base, uint32_t queue_ca
     m.bd = reinterpret_cast<float *>(m.qi + queue_cap);
     m.bi = reinterpret_cast<uint32_t *>(m.bd + kBuf);
     m.bk = m.bi + kBuf;
-    m.hrow = m.bk + kBuf;
-    m.cand = m.hrow + kCandGroup * kHeadWords;
-    m.pre = m.cand + kMaxM;
+    m.cand = m.bk + kBuf;
     return m;
 }
 
@@ -775,18 +769,10 @@ __device__ uint32_t flush(const SearchArgs &a, const WarpMem &m, uint32_t nb, ui
     return warp_merge<ORDER>(m, sz, L, cnt, a.orig, lane);
 }
 
-// Append this lane's fresh vertex (if any) to the buffer, flushing first when
-// a full chunk might not fit.
-template <int KIND, int ORDER, int CL, int STORE>
-__device__ __forceinline__ void append_fresh(const SearchArgs &a, const WarpMem &m, uint32_t &nb,
-                                             uint32_t *sz, uint32_t L, uint32_t &nk, uint32_t &n_dist,
-                                             bool fresh, uint32_t id, const Dist<KIND, CL, STORE> &D,
-                                             int lane) {
-    if (nb + 32 > kBuf) {
-        n_dist += nb;
-        nk = min(nk, flush<KIND, ORDER, CL, STORE>(a, m, nb, sz, L, true, D, lane));
-        nb = 0;
-    }
+// Append this lane's fresh vertex (if any) to the buffer. The caller makes
+// room first (one flush per group of candidates or batch of overflow
+// neighbours, so the kernel holds few inlined copies of flush).
+__device__ __forceinline__ void append_ids(const WarpMem &m, uint32_t &nb, bool fresh, uint32_t id, int lane) {
     const uint32_t bm = __ballot_sync(kFull, fresh);
     if (fresh) m.bi[nb + __popc(bm & lanemask_lt())] = id;
     nb += __popc(bm);
@@ -795,14 +781,13 @@ __device__ __forceinline__ void append_fresh(const SearchArgs &a, const WarpMem 
 
 // One query, run by one warp.
 template <int KIND, int ORDER, int CL, int STORE>
-__device__ void search_one(const SearchArgs &a, const WarpMem &m, uint32_t q, uint32_t slot, uint32_t *vis,
-                           uint32_t *dirty, int lane) {
+__device__ void search_one(const SearchArgs &a, const WarpMem &m, uint32_t q, uint32_t *vis, uint32_t *dirty,
+                           int lane) {
     uint32_t L = a.Lq ? __ldg(a.Lq + q) : a.L;
     // Init ids: n_lrn learned entries (m.cand) then n_plain of the init list.
     uint32_t n_lrn = 0, n_plain = L;
-    if (ORDER == ORDER_PANNS && a.mlp) {
-        const uint2 r = mlp_prologue(a.mlp, reinterpret_cast<const float *>(a.queries) + (size_t) q * CL * 32,
-                                     L, a.K, slot, q, m.cand, lane);
+    if (ORDER == ORDER_PANNS && a.decisions) {
+        const uint2 r = mlp_read_decision(a.decisions, a.dec_L_init, q, m.cand, lane);
         n_lrn = r.x & 0xffu;
         n_plain = r.x >> 8;
         L = r.y;
@@ -869,173 +854,123 @@ __device__ void search_one(const SearchArgs &a, const WarpMem &m, uint32_t q, ui
         n_expand += cnt;
         uint32_t nk = L;
         nb = 0;
-        for (uint32_t c0 = 0; c0 < cnt; c0 += kCandGroup) {
-            const uint32_t gc = min((uint32_t) kCandGroup, cnt - c0);
-            // Stage the head rows: one warp-wide 128-byte load per candidate,
-            // all issued before the first store.
-            // Lane j < gc also fetches candidate j's overflow offset (used if
-            // its row is longer than the head row), in flight with the rows.
-            const uint64_t my_off = (uint32_t) lane < gc ? __ldg(a.ovf_off + m.cand[c0 + lane]) : 0ull;
-#if PANNS_HEAD_REGS
-            // The head rows stay in registers: lane l holds word l of every
-            // candidate's row (word 0 the degree, words 1..31 neighbours), and
-            // the test-and-sets go by candidate, one row per chunk, so the
-            // neighbours keep their (candidate, slot) order.
-            uint32_t hv[kCandGroup], olds[kCandGroup];
-#pragma unroll
-            for (int j = 0; j < kCandGroup; ++j)
-                hv[j] = (uint32_t) j < gc ? __ldg(a.head + (size_t) m.cand[c0 + j] * kHeadWords + lane) : 0u;
-            uint32_t deg = 0, degsum = 0;
-#pragma unroll
-            for (int j = 0; j < kCandGroup; ++j) {
-                const uint32_t dj = __shfl_sync(kFull, hv[j], 0);  // 0 past the group
-                degsum += dj;
-                if (lane == j) deg = dj;
-                bool valid = lane >= 1 && (uint32_t) lane <= min(dj, (uint32_t) kHeadNbrs);
-                if (valid && hv[j] >= a.n) {
-                    atomicOr(a.error, ERR_BAD_ID);
-                    valid = false;
-                }
-                if (!valid) hv[j] = kFull;
-                olds[j] = visit_issue(vis, hv[j], valid);
+        // The step's work in units: the head rows of a group of up to
+        // kCandGroup candidates, then (if any of them is longer than its head
+        // row) batches of kOvfChunks * 32 overflow neighbours of the group.
+        // The fresh buffer is flushed at one place: before a unit that might
+        // not fit, and at the end of the step (the kernel then holds few
+        // inlined copies of flush, which keeps the hot loop's code compact).
+        uint32_t c0 = 0, gc = 0;              // the current group
+        uint64_t my_off = 0;                  // lane j < gc: candidate j's overflow offset
+        uint32_t oexcl = 0, ototal = 0, f0 = 0;
+        bool ovf = false;                     // overflow batches of the group left (warp-uniform)
+        for (;;) {
+            const bool done = !ovf && c0 >= cnt;
+            const uint32_t need = ovf ? 32u * kOvfChunks
+                                      : done ? (uint32_t) kBuf + 1u : min((uint32_t) kCandGroup, cnt - c0) * kHeadNbrs;
+            if (nb && nb + need > kBuf) {
+                n_dist += nb;
+                nk = min(nk, flush<KIND, ORDER, CL, STORE>(a, m, nb, &sz, L, true, D, lane));
+                nb = 0;
             }
-            n_edges += gc + degsum;
-            const bool any_long = __any_sync(kFull, deg > (uint32_t) kHeadNbrs);
-#pragma unroll
-            for (int j = 0; j < kCandGroup; ++j) {
-                if ((uint32_t) j >= gc) break;
-                const uint32_t id = hv[j];
-                const bool valid = id != kFull;
-                const bool fresh = valid && !(olds[j] & (1u << (id & 31)));
-                note_dirty(dirty, a.dirty_cap, dcount, valid && olds[j] == 0, id >> 5);
-                append_fresh<KIND, ORDER, CL, STORE>(a, m, nb, &sz, L, nk, n_dist, fresh, id, D, lane);
-            }
-#else
-            {
-                uint32_t hv[kCandGroup];
+            if (done) break;
+            if (!ovf) {
+                gc = min((uint32_t) kCandGroup, cnt - c0);
+                // The head rows: one warp-wide 128-byte load per candidate, all
+                // issued before any is used. Lane j < gc also fetches candidate
+                // j's overflow offset (used if its row is longer than the head row).
+                my_off = (uint32_t) lane < gc ? __ldg(a.ovf_off + m.cand[c0 + lane]) : 0ull;
+                // The head rows stay in registers: lane l holds word l of every
+                // candidate's row (word 0 the degree, words 1..31 neighbours), and
+                // the test-and-sets go by candidate, one row per chunk, so the
+                // neighbours keep their (candidate, slot) order.
+                uint32_t hv[kCandGroup], olds[kCandGroup];
 #pragma unroll
                 for (int j = 0; j < kCandGroup; ++j)
-                    hv[j] = (uint32_t) j < gc ? __ldg(a.head + (size_t) m.cand[c0 + j] * kHeadWords + lane)
-                                              : 0u;
+                    hv[j] = (uint32_t) j < gc ? __ldg(a.head + (size_t) m.cand[c0 + j] * kHeadWords + lane) : 0u;
+                uint32_t deg = 0, degsum = 0;
 #pragma unroll
-                for (int j = 0; j < kCandGroup; ++j)
-                    if ((uint32_t) j < gc) m.hrow[j * kHeadWords + lane] = hv[j];
-            }
-            __syncwarp();
-            // Prefix sums of the head-row neighbour counts.
-            uint32_t deg = 0, hcount = 0;
-            if (lane < (int) gc) {
-                deg = m.hrow[lane * kHeadWords];
-                hcount = min(deg, (uint32_t) kHeadNbrs);
-            }
-            uint32_t incl = hcount;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t t = __shfl_up_sync(kFull, incl, o);
-                if (lane >= o) incl += t;
-            }
-            const uint32_t total = __shfl_sync(kFull, incl, 31);
-            // Start of each candidate's neighbours in the flattened list, in
-            // registers of every lane (lanes >= gc hold total, past every f).
-            uint32_t pre_r[kCandGroup];
-#pragma unroll
-            for (int t = 0; t < kCandGroup; ++t) pre_r[t] = __shfl_sync(kFull, incl - hcount, t);
-            uint32_t degsum = deg;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) degsum += __shfl_xor_sync(kFull, degsum, o);
-            n_edges += gc + degsum;
-            const bool any_long = __any_sync(kFull, deg > (uint32_t) kHeadNbrs);
-            __syncwarp();
-            // Head-row neighbours in (candidate, slot) order: every visited
-            // test-and-set of the group is issued before any result is used.
-            uint32_t ids[kGroupChunks], olds[kGroupChunks];
-#pragma unroll
-            for (int ch = 0; ch < kGroupChunks; ++ch) {
-                const uint32_t f = ch * 32 + lane;
-                uint32_t id = 0;
-                bool valid = f < total;
-                if (valid) {
-                    uint32_t j = 0, pj = 0;  // owner: the last candidate starting at or before f
-#pragma unroll
-                    for (int t = 1; t < kCandGroup; ++t)
-                        if (pre_r[t] <= f) {
-                            j = t;
-                            pj = pre_r[t];
-                        }
-                    id = m.hrow[j * kHeadWords + 1 + (f - pj)];
-                    if (id >= a.n) {
+                for (int j = 0; j < kCandGroup; ++j) {
+                    const uint32_t dj = __shfl_sync(kFull, hv[j], 0);  // 0 past the group
+                    degsum += dj;
+                    if (lane == j) deg = dj;
+                    bool valid = lane >= 1 && (uint32_t) lane <= min(dj, (uint32_t) kHeadNbrs);
+                    if (valid && hv[j] >= a.n) {
                         atomicOr(a.error, ERR_BAD_ID);
                         valid = false;
                     }
+                    if (!valid) hv[j] = kFull;
+                    olds[j] = visit_issue(vis, hv[j], valid);
                 }
-                ids[ch] = valid ? id : kFull;
-                olds[ch] = visit_issue(vis, id, valid);
-            }
+                n_edges += gc + degsum;
 #pragma unroll
-            for (int ch = 0; ch < kGroupChunks; ++ch) {
-                if (ch * 32 >= (int) total) break;
-                const uint32_t id = ids[ch];
-                const bool valid = id != kFull;
-                const bool fresh = valid && !(olds[ch] & (1u << (id & 31)));
-                note_dirty(dirty, a.dirty_cap, dcount, valid && olds[ch] == 0, id >> 5);
-                append_fresh<KIND, ORDER, CL, STORE>(a, m, nb, &sz, L, nk, n_dist, fresh, id, D, lane);
-            }
-#endif
-            // Rows longer than the head row: the rest from the overflow lists
-            // of all the group's long candidates, flattened in (candidate,
-            // slot) order; per batch of kOvfChunks * 32 every load is issued
-            // before any test-and-set, and every test-and-set before any
-            // result is used.
-            if (any_long) {
-                const uint32_t ocount = deg > (uint32_t) kHeadNbrs ? deg - kHeadNbrs : 0u;  // 0 for lanes >= gc
-                uint32_t oincl = ocount;
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const uint32_t t = __shfl_up_sync(kFull, oincl, o);
-                    if (lane >= o) oincl += t;
+                for (int j = 0; j < kCandGroup; ++j) {
+                    if ((uint32_t) j >= gc) break;
+                    const uint32_t id = hv[j];
+                    const bool valid = id != kFull;
+                    const bool fresh = valid && !(olds[j] & (1u << (id & 31)));
+                    note_dirty(dirty, a.dirty_cap, dcount, valid && olds[j] == 0, id >> 5);
+                    append_ids(m, nb, fresh, id, lane);
                 }
-                const uint32_t ototal = __shfl_sync(kFull, oincl, 31);
-                const uint32_t oexcl = oincl - ocount;
-                for (uint32_t f0 = 0; f0 < ototal; f0 += 32 * kOvfChunks) {
-                    uint32_t oid[kOvfChunks], oold[kOvfChunks];
+                // Rows longer than the head row: the rest from the overflow
+                // lists of all the group's long candidates, flattened in
+                // (candidate, slot) order, in the batches that follow.
+                if (__any_sync(kFull, deg > (uint32_t) kHeadNbrs)) {
+                    const uint32_t ocount = deg > (uint32_t) kHeadNbrs ? deg - kHeadNbrs : 0u;  // 0 for lanes >= gc
+                    uint32_t oincl = ocount;
 #pragma unroll
-                    for (int ch = 0; ch < kOvfChunks; ++ch) {
-                        const uint32_t f = f0 + ch * 32 + lane;
-                        // owner: the last candidate whose flattened range starts at or before f
-                        uint32_t j = 0;
-                        for (uint32_t t = 1; t < gc; ++t)
-                            if (__shfl_sync(kFull, oexcl, t) <= f) j = t;
-                        const uint32_t pj = __shfl_sync(kFull, oexcl, j);
-                        const uint64_t offj = __shfl_sync(kFull, my_off, j);
-                        oid[ch] = f < ototal ? __ldg(a.ovf + offj + (f - pj)) : kFull;
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const uint32_t t = __shfl_up_sync(kFull, oincl, o);
+                        if (lane >= o) oincl += t;
                     }
+                    ototal = __shfl_sync(kFull, oincl, 31);
+                    oexcl = oincl - ocount;
+                    f0 = 0;
+                    ovf = true;
+                } else {
+                    c0 += kCandGroup;
+                }
+            } else {
+                // One overflow batch: every load is issued before any
+                // test-and-set, and every test-and-set before any result is used.
+                uint32_t oid[kOvfChunks], oold[kOvfChunks];
 #pragma unroll
-                    for (int ch = 0; ch < kOvfChunks; ++ch) {
-                        bool valid = oid[ch] != kFull;
-                        if (valid && oid[ch] >= a.n) {
-                            atomicOr(a.error, ERR_BAD_ID);
-                            valid = false;
-                            oid[ch] = kFull;
-                        }
-                        oold[ch] = visit_issue(vis, oid[ch], valid);
-                    }
+                for (int ch = 0; ch < kOvfChunks; ++ch) {
+                    const uint32_t f = f0 + ch * 32 + lane;
+                    // owner: the last candidate whose flattened range starts at or before f
+                    uint32_t j = 0;
+                    for (uint32_t t = 1; t < gc; ++t)
+                        if (__shfl_sync(kFull, oexcl, t) <= f) j = t;
+                    const uint32_t pj = __shfl_sync(kFull, oexcl, j);
+                    const uint64_t offj = __shfl_sync(kFull, my_off, j);
+                    oid[ch] = f < ototal ? __ldg(a.ovf + offj + (f - pj)) : kFull;
+                }
 #pragma unroll
-                    for (int ch = 0; ch < kOvfChunks; ++ch) {
-                        if (f0 + ch * 32 >= ototal) break;
-                        const uint32_t id = oid[ch];
-                        const bool valid = id != kFull;
-                        const bool fresh = valid && !(oold[ch] & (1u << (id & 31)));
-                        note_dirty(dirty, a.dirty_cap, dcount, valid && oold[ch] == 0, id >> 5);
-                        append_fresh<KIND, ORDER, CL, STORE>(a, m, nb, &sz, L, nk, n_dist, fresh, id, D, lane);
+                for (int ch = 0; ch < kOvfChunks; ++ch) {
+                    bool valid = oid[ch] != kFull;
+                    if (valid && oid[ch] >= a.n) {
+                        atomicOr(a.error, ERR_BAD_ID);
+                        valid = false;
+                        oid[ch] = kFull;
                     }
+                    oold[ch] = visit_issue(vis, oid[ch], valid);
+                }
+#pragma unroll
+                for (int ch = 0; ch < kOvfChunks; ++ch) {
+                    if (f0 + ch * 32 >= ototal) break;
+                    const uint32_t id = oid[ch];
+                    const bool valid = id != kFull;
+                    const bool fresh = valid && !(oold[ch] & (1u << (id & 31)));
+                    note_dirty(dirty, a.dirty_cap, dcount, valid && oold[ch] == 0, id >> 5);
+                    append_ids(m, nb, fresh, id, lane);
+                }
+                f0 += 32 * kOvfChunks;
+                if (f0 >= ototal) {
+                    ovf = false;
+                    c0 += kCandGroup;
                 }
             }
             __syncwarp();
-        }
-        if (nb) {
-            n_dist += nb;
-            nk = min(nk, flush<KIND, ORDER, CL, STORE>(a, m, nb, &sz, L, true, D, lane));
-            nb = 0;
         }
         k = nk <= last_k ? nk : last_k + 1;
     }
@@ -1076,7 +1011,7 @@ __global__ void __launch_bounds__(128, PANNS_SEARCH_MIN_BLOCKS) search_kernel(Se
         if (lane == 0) q = atomicAdd(a.counter, 1u);
         q = __shfl_sync(kFull, q, 0);
         if (q >= a.nq) break;
-        search_one<KIND, ORDER, CL, STORE>(a, m, q, slot, vis, dirty, lane);
+        search_one<KIND, ORDER, CL, STORE>(a, m, q, vis, dirty, lane);
     }
 }
 

@@ -15,7 +15,8 @@ include/panns_learned.h):
    1 L output), BF16 weights, float32 accumulation, by the library's own
    forward / backward kernels.
 4. ``attach``: hands the network and representatives to an ``Index``;
-   searches with ``flags=FLAG_LEARNED`` then run it in the kernel prologue,
+   searches with ``flags=FLAG_LEARNED`` then run it batched before the search
+   kernel and start each query from its decision,
    and queries whose top softmax probability is below ``min_conf`` run the
    plain search (PANNS init list, the call's L).
 """

@@ -5,7 +5,7 @@
   that oracle) to float32 accumulation error.
 * Training lowers the loss; k-means returns distinct representatives that
   lie in their own cells.
-* The learned search is exact given its decisions: the prologue's per-query
+* The learned search is exact given its decisions: the batched inference's per-query
   decision (fallback, queue length, entry vertices) matches the oracle's, and
   the ids equal the oracle's top-M search from those entries; with a network
   that is never confident, every query runs the plain search, id for id.
