@@ -297,7 +297,7 @@ def bench_ours(args):
     # The learned entry / L-budget network (trained on the GPU on held-out
     # queries; rank 0 builds it, the others load the cached file).
     model = None
-    if not args.no_learned and not fixed:
+    if not args.no_learned and (not fixed or args.entries):
         if rank == 0:
             model = workloads.learned_model(spec, handles[N.STORE_BF16], log=log)
         barrier()
@@ -317,7 +317,12 @@ def bench_ours(args):
     if fixed:
         c = {"storage": args.storage or 0, "M": args.M, "L": args.L, "warps_per_block": args.wpb,
              "learned": None, "blocks_per_sm": 0, "warps_per_query": 1}
-        choices = {"plain": dict(c, storage=0), "head": c, "tables": []}
+        if args.entries:
+            parts = args.entries.split(":")
+            c["learned"] = {"E": int(parts[0]), "L_init": int(parts[1]), "use_L": False}
+            if len(parts) > 2:
+                c["learned"]["min_conf"] = float(parts[2])
+        choices = {"plain": dict(c, storage=0, learned=None), "head": c, "tables": []}
     elif rank == 0:
         t0 = time.time()
         plain = AT.tune(handles[N.STORE_FP32], tune_q, tune_gt, K=K, target=RECALL_TARGET,
@@ -662,6 +667,8 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="leave the learned entry network out")
     ap.add_argument("--no-parity", action="store_true", help="skip the id check against the reference")
     ap.add_argument("--wpb", type=int, default=2, help="warps per block with a fixed --L and --M")
+    ap.add_argument("--entries", default=None,
+                    help="with a fixed --L and --M: learned entries E:L_init[:min_conf] (the network is trained first)")
     ap.add_argument("--workload", default="mixture_1m_d96", choices=["mixture_1m_d96", "u8_1m_d128", "mixture_10m_d96"],
                     help="mixture_1m_d96: the batched-FP32 config (default); u8_1m_d128: the "
                          "reduced-precision config's integer-valued d = 128 variant (R = 64); mixture_10m_d96: "
