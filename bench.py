@@ -266,6 +266,10 @@ def bench_ours(args):
 
     spec = workloads.SPECS[args.workload](**({"n": args.n} if args.n else {}), nq=args.nq * world)
     args.n = spec["n"]
+    if spec.get("large"):
+        if world > 1:
+            raise SystemExit(f"workload {args.workload}: one GPU only (the whole index on each replica)")
+        return bench_large(args, spec)
     fixed = bool(args.L and args.M)  # a given operating point: no tuning set, no autotuning
     if rank == 0:
         W = workloads.build(spec, device=f"cuda:{local}", log=log)
@@ -433,6 +437,8 @@ def bench_ours(args):
             if wq == head.warps_per_query and head.learned is None:
                 continue  # the head itself
             options.append((wq, ixh, dict(kw, flags=N.FLAG_CUDA_GRAPH, warps_per_query=wq)))
+            if head.learned is not None and wq != head.warps_per_query:  # the network with several warps
+                options.append((wq, ixh, dict(kw, flags=kw["flags"] | N.FLAG_CUDA_GRAPH, warps_per_query=wq)))
         if head.storage != N.STORE_FP32:  # and the float32 rows with several warps
             for wq in (2, 4, 8):
                 options.append((wq, handles[N.STORE_FP32],
@@ -451,7 +457,8 @@ def bench_ours(args):
             ms = e0.elapsed_time(e1)
             r_ = {"qps": round(nb * B / (ms / 1e3), 1), "ms_per_batch": round(ms / nb, 4), "warps_per_query": wq,
                   "storage": names[kwb["storage"]]}
-            tried[f"{wq}/{names[kwb['storage']]}"] = r_["qps"]
+            r_["learned"] = bool(kwb["flags"] & N.FLAG_LEARNED)
+            tried[f"{wq}/{names[kwb['storage']]}" + ("+learned" if r_["learned"] else "")] = r_["qps"]
             if best_b is None or r_["qps"] > best_b["qps"]:
                 best_b = r_
         batching[str(B)] = dict(best_b, qps_by_warps_per_query=tried)
@@ -548,6 +555,186 @@ def bench_ours(args):
         ixx.close()
     if world > 1:
         dist.destroy_process_group()
+
+
+def bench_large(args, spec):
+    """The large uneven-batch configuration on one GPU, held in memory: base
+    drawn on the GPU, the cell-restricted graph, one handle with the float32
+    rows and a BF16 copy, float64 ground truth, the learned network, the
+    autotuner's head (BF16 +- network) against plain FP32, then batches of
+    1 ... 65,536 queries at the head's configuration and at L = 200 and 400."""
+    import numpy as np
+    import torch
+
+    from parallel_anns_b200 import autotune as AT
+    from parallel_anns_b200 import learned as LE
+    from parallel_anns_b200 import native as N
+    from parallel_anns_b200 import workloads
+    from parallel_anns_b200.searching import Index, ground_truth as gpu_gt, recall
+
+    K, nq, d = 100, args.nq, spec["d"]
+    tm = {}
+    t0 = time.time()
+    base = workloads.vectors(spec, spec["n"], spec["base_seed"])
+    qs = workloads.vectors(spec, nq, spec["query_seed"])
+    tune_q = workloads.vectors(spec, 10_000, spec["query_seed"] + 1)
+    tm["generate_s"] = round(time.time() - t0, 1)
+    t0 = time.time()
+    g = workloads.build_graph(base, spec)
+    tm["graph_s"] = round(time.time() - t0, 1)
+    ginfo = {"entry": int(g.entry), "width": int(g.width), "avg_degree": round(g.nbrs.size / g.n, 2),
+             "repaired": int(getattr(g, "repaired", 0)), "cells": spec["cells"], "probe": spec["probe"]}
+    log(f"graph: {ginfo} in {tm['graph_s']} s")
+    t0 = time.time()
+    ix = Index(0)
+    ix.set_base(base, storage=N.STORE_BF16)
+    ix.set_graph(g)
+    del g
+    ix.set_queries(qs)
+    gts, _ = gpu_gt(ix, qs, K)
+    tune_gt, _ = gpu_gt(ix, tune_q, K)
+    tm["index_and_ground_truth_s"] = round(time.time() - t0, 1)
+    model = None
+    if not args.no_learned:
+        t0 = time.time()
+        # One representative per mixture component, and trace labels from a
+        # queue long enough to hold every neighbour of the entry (the
+        # components meet only there).
+        model = LE.build_model(ix, workloads.vectors(spec, 200_000, spec["base_seed"] + 2000), R=spec["reps"],
+                               K=K, M=8, L_ref=max(1000, ginfo["width"] + 1000), T=10, epochs=10, batch=1024,
+                               lr=2e-3, lam=1.0, seed=0, kmeans_iters=8, log=log)
+        tm["learned_s"] = round(time.time() - t0, 1)
+    learned_opts = [dict(E=8, L_init=8, use_L=False), dict(E=16, L_init=16, use_L=False, min_conf=0.5)]
+    t0 = time.time()
+    Ms = [args.M] if args.M else M_SWEEP
+    plain = AT.tune(ix, tune_q, tune_gt, K=K, target=RECALL_TARGET, storages=(N.STORE_FP32,), Ms=Ms, wpbs=(2, 4),
+                    log=log)
+    head = AT.tune(ix, tune_q, tune_gt, K=K, target=RECALL_TARGET, storages=(N.STORE_BF16,), Ms=Ms, wpbs=(2, 4),
+                   learned_model=model, learned_opts=learned_opts if model is not None else (), log=log)
+    tm["autotune_s"] = round(time.time() - t0, 1)
+    if plain.kernel_ms < head.kernel_ms:
+        head = plain
+    if head.learned is not None:
+        LE.attach(ix, model, **head.learned)
+    log(f"plain fp32 L={plain.L} M={plain.M} {plain.kernel_ms:.3f} ms; head storage={head.storage} L={head.L} "
+        f"M={head.M} learned={head.learned} {head.kernel_ms:.3f} ms")
+
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    sampler = ClockSampler(0)
+
+    def timed(c):
+        kw = c.search_kwargs()
+        for _ in range(args.warmup):
+            ix.search(K=K, **kw)
+        torch.cuda.synchronize()
+        kms, tot_, ids_ = 0.0, {"n_dist": 0, "n_edges": 0}, None
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            ids_, st = ix.search(K=K, **kw)
+            kms += st["kernel_ms"]
+            for k_ in tot_:
+                tot_[k_] += st[k_]
+        torch.cuda.synchronize()
+        return kms, tot_, ids_
+
+    sampler.start()
+    kernel_ms, tot, last_ids = timed(head)
+    rec = recall(last_ids, gts, 100, 100)
+    if head is plain:
+        p_ms, p_tot, p_ids = kernel_ms, tot, last_ids
+    else:
+        p_ms, p_tot, p_ids = timed(plain)
+    p_rec = recall(p_ids, gts, 100, 100)
+    # End to end through the host-pointer call, pinned queries and ids.
+    kw = head.search_kwargs()
+    q_pin = torch.from_numpy(qs).pin_memory().numpy()
+    out_pin = torch.empty((nq, K), dtype=torch.int32).pin_memory().numpy().view(np.uint32)
+    for _ in range(args.warmup):
+        ix.search(q_pin, K=K, out=out_pin, **kw)
+    e2e_s = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ix.search(q_pin, K=K, out=out_pin, **kw)
+        e2e_s += time.perf_counter() - t0
+    clocks = sampler.stop()
+
+    # Uneven batches through the asynchronous device-pointer entry point with
+    # the CUDA-graph-captured launch, back to back on one stream, at the
+    # head's configuration and at L = 200 and 400 (recall of each L on the
+    # evaluation queries).
+    pool = torch.from_numpy(workloads.vectors(spec, 65_536, spec["query_seed"] + 7)).cuda()
+    stream = torch.cuda.Stream()
+    batches = {}
+    for Lb in sorted({head.L, 200, 400}):
+        # warps per query chosen by the library from the batch size
+        kwb = dict(kw, L=Lb, flags=kw["flags"] | N.FLAG_CUDA_GRAPH, warps_per_query=0, warps_per_block=0,
+                   blocks_per_sm=0)
+        ids_b, _ = ix.search(K=K, **dict(kw, L=Lb))
+        row = {"recall100": round(recall(ids_b, gts, 100, 100), 5)}
+        for B in (1, 16, 256, 4096, 65_536):
+            nb = max(2, min(200, 131_072 // B))
+            outb = torch.empty((B, K), dtype=torch.int32, device="cuda")
+            for i in range(2):
+                s0 = (i * B) % (65_536 - B + 1)
+                ix.search_device(pool[s0:s0 + B], outb, K=K, stream=stream, **kwb)
+            stream.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for i in range(nb):
+                s0 = (i * B) % (65_536 - B + 1)
+                ix.search_device(pool[s0:s0 + B], outb, K=K, stream=stream, **kwb)
+            e1.record(stream)
+            stream.synchronize()
+            ms = e0.elapsed_time(e1)
+            row[str(B)] = round(nb * B / (ms / 1e3), 1)
+        batches[f"L{Lb}"] = row
+    log(f"batches: {batches}")
+
+    steps = args.steps
+    s_el = {N.STORE_FP32: 4, N.STORE_BF16: 2, N.STORE_FP8: 1}[head.storage]
+    alg_bytes = (tot["n_dist"] * (s_el * d + 4) + 4 * tot["n_edges"]) / steps + nq * (4 * d + 4 * K)
+    if head.storage != N.STORE_FP32:
+        alg_bytes += nq * head.L * (4 * d + 4)
+    achieved = alg_bytes / (kernel_ms / steps / 1e3) / 1e9
+    p_alg = (p_tot["n_dist"] * (4 * d + 4) + 4 * p_tot["n_edges"]) / steps + nq * (4 * d + 4 * K)
+    peak, peak_kind = measured_peak_hbm()
+    names = {N.STORE_FP32: "fp32", N.STORE_BF16: "bf16", N.STORE_FP8: "fp8"}
+    why = ("not run at this size: the reference's loaders build the whole index in host memory "
+           "(load_nsg_graph interleaves ~600 B rows: ~60 GB, next to the 38 GB base), and its "
+           "all-pairs tools cannot build this graph")
+    line = {
+        "metric": metric_for(spec), "value": round(nq * steps / (kernel_ms / 1e3), 1), "unit": UNIT, "n_gpus": 1,
+        "steps": steps, "warmup": args.warmup, "ms_per_step": round(kernel_ms / steps, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": names[head.storage],
+        "data": "synthetic",
+        "config": {"workload": "batched search, " + workloads.describe(spec) + " (per GPU), in memory",
+                   "graph": dict(ginfo, rule="exact 64-NN within each k-means cell and its 3 nearest cells, "
+                                            "MRNG prune to R=48, reverse edges up to R, medoid entry, "
+                                            "reachability repair"),
+                   "L": head.L, "M": head.M, "warps_per_block": head.warps_per_block,
+                   "storage": names[head.storage], "accumulate": "f32",
+                   "rerank": "exact f32 of the final L" if head.storage != N.STORE_FP32 else None,
+                   "learned": head.learned, "recall100": round(rec, 5),
+                   "operating_point": "autotuned on 10k held-out queries",
+                   "l2": "inputs > L2 and a 256 MB L2 flush before each step", "build_s": tm},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": None, "peak_source": peak_kind},
+        "e2e": {"value": round(nq * steps / e2e_s, 1), "unit": UNIT, "h2d_bytes_per_step": nq * d * 4,
+                "d2h_bytes_per_step": nq * K * 4 + nq * 16 + 4},
+        "gpu_launches": steps,
+        "plain_fp32": {"value": round(nq * steps / (p_ms / 1e3), 1), "L": plain.L, "M": plain.M,
+                       "recall100": round(p_rec, 5),
+                       "roofline_frac": round(p_alg / (p_ms / steps / 1e3) / 1e9 / peak, 4)},
+        "uneven_batches_qps": batches,
+        "parity": {"unavailable": why},
+        "clocks": clocks,
+        "cpu_baseline": {"unavailable": why},
+    }
+    print(json.dumps(line), flush=True)
+    ix.close()
 
 
 def cpu_baseline(paths, L, nq_total, log):
@@ -669,7 +856,8 @@ def main():
     ap.add_argument("--wpb", type=int, default=2, help="warps per block with a fixed --L and --M")
     ap.add_argument("--entries", default=None,
                     help="with a fixed --L and --M: learned entries E:L_init[:min_conf] (the network is trained first)")
-    ap.add_argument("--workload", default="mixture_1m_d96", choices=["mixture_1m_d96", "u8_1m_d128", "mixture_10m_d96"],
+    ap.add_argument("--workload", default="mixture_1m_d96",
+                    choices=["mixture_1m_d96", "u8_1m_d128", "mixture_10m_d96", "mixture_100m_d96"],
                     help="mixture_1m_d96: the batched-FP32 config (default); u8_1m_d128: the "
                          "reduced-precision config's integer-valued d = 128 variant (R = 64); mixture_10m_d96: "
                          "the learned-entry config's 10M base")

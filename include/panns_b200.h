@@ -90,8 +90,9 @@ typedef struct {
                                 but no more than fit in 196 KB of shared memory */
     uint32_t warps_per_query; /* 1: one warp per query (warps_per_block queries per block);
                                  2, 4 or 8: that many warps share each query's steps (one query per
-                                 block; NSG_SEQ, TOP_M, PSS_V5 at T = 1, any storage, no learned
-                                 prologue), for small batches and long queues; same ids and counts.
+                                 block; NSG_SEQ, TOP_M, PSS_V5 at T = 1, any storage, with or
+                                 without PANNS_FLAG_LEARNED), for small batches and long queues; same
+                                 ids and counts.
                                  0: chosen from nq and L (8 up to one query per SM or for L >= 2048,
                                  2 up to ten per SM, else 1) when the mode allows it and
                                  warps_per_block and blocks_per_sm are 0, else 1 */

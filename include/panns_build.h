@@ -49,6 +49,30 @@ int panns_build_nsg(int device, const float *base, uint32_t n, uint32_t d, uint3
 int panns_build_nsg_ex(int device, const float *base, uint32_t n, uint32_t d, uint32_t knn_k, uint32_t R,
                        uint32_t screen, panns_graph **out);
 
+/* The construction of the large-graph configuration (100M vectors on one GPU,
+ * where all pairs are out of reach): the vertices are partitioned into
+ * `cells` k-means cells (Lloyd, `iters` rounds from `cells` distinct rows
+ * chosen by `seed`, on `sample` rows taken at a fixed stride; then every
+ * vertex goes to its nearest centroid), and the k-NN list of vertex a holds
+ * the knn_k vertices b != a with the smallest (d64(a, b), b) among the
+ * members of a's cell and of the `probe` cells whose centroids are nearest to
+ * it (by float64 squared distance, then index). The candidates come from a
+ * float32 screen keeping k + 8 per row, ranked exactly in float64; prune,
+ * entry and repair are those of panns_build_nsg. probe <= 8; a list with
+ * fewer than knn_k candidates is shorter. With `reverse` set, before the
+ * repair every pruned edge a -> b (a ascending, then list order) also gives
+ * b -> a while b has fewer than R neighbours and not a already (the part
+ * efanna2e's InterInsert plays), which keeps tight, far-apart clusters
+ * navigable from inside. panns_graph_cells returns the partition. This
+ * plays the part of the reference's k-NN graph input
+ * (IndexNSG::Load_nn_graph) for sizes its all-pairs tools cannot build. */
+int panns_build_nsg_cells(int device, const float *base, uint32_t n, uint32_t d, uint32_t knn_k, uint32_t R,
+                          uint32_t cells, uint32_t probe, uint32_t sample, uint32_t iters, uint32_t seed,
+                          uint32_t reverse, panns_graph **out);
+/* The partition of a graph built by panns_build_nsg_cells (each pointer
+ * optional): number of cells, probe, the cell of every vertex (n), and each
+ * cell's probe nearest cells (cells x probe; ~0 where there are fewer). */
+int panns_graph_cells(const panns_graph *g, uint32_t *cells, uint32_t *probe, uint32_t *cell, uint32_t *near);
 /* Sizes of a built graph (each pointer optional): vertices, largest degree,
  * entry vertex, total adjacency entries, in-edges added by the repair. */
 int panns_graph_info(const panns_graph *g, uint32_t *n, uint32_t *width, uint32_t *entry, uint64_t *n_edges,

@@ -4,7 +4,7 @@ INFRASTRUCTURE ONLY (imported by tests/ to check the GPU results, never by the p
 Restates, in float64 numpy, the network, loss and gradient that the GPU
 kernels of parallel_anns_b200/csrc/learned.cu compute (the parameter layout
 and loss of include/panns_learned.h), and the per-query decision of the
-search-kernel prologue (parallel_anns_b200/csrc/mlp_infer.cuh). The weight
+batched inference (decide_kernel in parallel_anns_b200/csrc/learned.cu). The weight
 matrices are rounded to BF16 (round to nearest, ties to even) exactly as the
 GPU rounds them; everything else is float64 here and float32 on the GPU, so
 the two agree to float32 accumulation error. No reference counterpart exists
@@ -113,7 +113,7 @@ def numeric_grad(params, X, cells, y, d, R, lam, idx, h=1e-6):
 
 
 def decide(params, X, d, R, reps, *, E, L_init, L_min, use_L, L_scale, min_conf, K, L, L_exp=1.0):
-    """The prologue's per-query decision: (fallback, L_q, entries, n_plain,
+    """The per-query decision of the batched inference: (fallback, L_q, entries, n_plain,
     confidence, regressor output, logits)."""
     _, _, Z, _ = forward(params, X, d, R, True)
     out = []

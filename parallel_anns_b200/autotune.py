@@ -104,8 +104,7 @@ def tune(index, queries, gt, *, K=100, target=0.95, storages=(N.STORE_FP32,), Ms
                         lo = mid + 1
                 L = L_grid[lo]
                 shapes = [(w, bps, 1) for w in wpbs for bps in bpss]
-                if opt is None:  # several warps per query: without the learned network
-                    shapes += [(wq, 0, wq) for wq in wpqs if wq > 1]
+                shapes += [(wq, 0, wq) for wq in wpqs if wq > 1]  # several warps per query
                 for w, bps, wq in shapes:
                     # blocks_per_sm counts blocks of w warps: keep the warps per SM comparable
                     b = bps * 4 // w if bps else 0

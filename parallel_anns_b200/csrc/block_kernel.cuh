@@ -37,7 +37,8 @@ __host__ __device__ inline uint32_t block_smem_bytes(uint32_t queue_cap, uint32_
            + kBlockCtl * 4u;                                          // control words
 }
 
-enum { BC_Q = 0, BC_SZ, BC_CNT, BC_LASTK, BC_K, BC_NK, BC_DIRTY, BC_DIST, BC_EDGES, BC_SEG };  // BC_SEG + w, w < W <= 8
+enum { BC_Q = 0, BC_SZ, BC_CNT, BC_LASTK, BC_K, BC_NK, BC_DIRTY, BC_DIST, BC_EDGES, BC_LRN, BC_LQ,
+       BC_SEG };  // BC_SEG + w, w < W <= 8
 
 // Number of elements of the sorted list (d, k)[0..n) that precede (dv, kv).
 __device__ __forceinline__ uint32_t list_rank(const float *d, const uint32_t *k, uint32_t n, float dv, uint32_t kv) {
@@ -73,7 +74,23 @@ __device__ void block_search_one(const SearchArgs &a, uint32_t q, uint8_t *smem,
     uint32_t *hrow = hrowAll + w * kCandGroup * kHeadWords;
     uint32_t *pre = preAll + w * 64;
 
-    const uint32_t L = a.Lq ? __ldg(a.Lq + q) : a.L;
+    uint32_t L = a.Lq ? __ldg(a.Lq + q) : a.L;
+    // Init ids: n_lrn learned entries (cand) then n_plain of the init list.
+    uint32_t n_lrn = 0, n_plain = L;
+    if (a.decisions) {
+        if (w == 0) {
+            const uint2 r = mlp_read_decision(a.decisions, a.dec_L_init, q, cand, lane);
+            if (lane == 0) {
+                ctl[BC_LRN] = r.x;
+                ctl[BC_LQ] = r.y;
+            }
+        }
+        __syncthreads();
+        n_lrn = ctl[BC_LRN] & 0xffu;
+        n_plain = ctl[BC_LRN] >> 8;
+        L = ctl[BC_LQ];
+    }
+    const uint32_t n_init = n_lrn + n_plain;
     Dist<KIND, CL, STORE> D;
     D.load(a, q, lane);
     if (tid == 0) {
@@ -189,15 +206,16 @@ __device__ void block_search_one(const SearchArgs &a, uint32_t q, uint8_t *smem,
         if (lane == 0) ctl[BC_SEG + w] = cnt;
     };
 
-    // Initial queue: the L init ids, W * kBuf at a time.
+    // Initial queue: the init ids (learned entries first, a repeated id
+    // entering once), W * kBuf at a time.
     const uint32_t *init = a.init_ids + (size_t) q * a.init_stride;
-    for (uint32_t r0 = 0; r0 < L; r0 += W * kBuf) {
+    for (uint32_t r0 = 0; r0 < n_init; r0 += W * kBuf) {
         uint32_t nb = 0;
-        const uint32_t lo = r0 + w * kBuf, hi = min(L, lo + kBuf);
+        const uint32_t lo = r0 + w * kBuf, hi = min(n_init, lo + kBuf);
         for (uint32_t i0 = lo; i0 < hi; i0 += 32) {
             const uint32_t i = i0 + lane;
             const bool valid = i < hi;
-            const uint32_t id = valid ? __ldg(init + i) : 0u;
+            const uint32_t id = valid ? (i < n_lrn ? cand[i] : __ldg(init + (i - n_lrn))) : 0u;
             const bool ok = valid && id < a.n;
             if (valid && !ok) atomicOr(a.error, ERR_BAD_INIT);
             const uint32_t old = visit_issue(vis, id, ok);

@@ -15,6 +15,10 @@ struct panns_graph {
     std::vector<uint32_t> knn;  // n x k (kept for the repair and for callers)
     uint32_t k = 0;
     uint32_t repaired = 0;
+    // Cell-restricted construction only: each vertex's cell and each cell's
+    // `probe` nearest cells (cells x probe).
+    uint32_t cells = 0, probe = 0;
+    std::vector<uint32_t> cell, near;
 };
 
 namespace panns {

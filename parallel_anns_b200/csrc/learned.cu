@@ -15,6 +15,7 @@
 #include <numeric>
 #include <random>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/panns_learned.h"
@@ -70,15 +71,18 @@ __device__ __forceinline__ void mma_tf32(float (&c)[4], const uint32_t (&a)[4], 
 
 // C[M x N] = A(M x K) * B(K x N) (+ bias[n]) (relu) (or C += when accumulate).
 // A(m, k) = AT ? A[k * lda + m] : A[m * lda + k]; B(k, n) = BT ? B[n * ldb + k]
-// : B[k * ldb + n]. 64 x 64 tiles staged through shared memory 16 deep, the
-// products on the tensor cores (split TF32, float32 accumulation); the order
-// of every sum is fixed, so results are deterministic.
+// : B[k * ldb + n]. 64 x 64 tiles staged through shared memory 32 deep, the
+// next slice's loads in flight (registers) while the tensor cores work on the
+// current one (split TF32, float32 accumulation); the order of every sum is
+// fixed (k ascending in steps of 8), so results are deterministic.
 template <typename TA, typename TB, bool AT, bool BT>
 __global__ void __launch_bounds__(256) gemm_kernel(const TA *__restrict__ A, int lda, const TB *__restrict__ B,
                                                    int ldb, float *__restrict__ C, int ldc, int M, int N, int K,
                                                    const float *__restrict__ bias, int relu, int accumulate) {
-    __shared__ float As[16][64 + 4];
-    __shared__ float Bs[16][64 + 4];
+    constexpr int BK = 32;
+    constexpr bool kBExact = std::is_same<TB, __nv_bfloat16>::value;  // BF16 is exact in TF32
+    __shared__ float As[2][BK][64 + 4];
+    __shared__ float Bs[2][BK][64 + 4];
     const int tid = threadIdx.x;
     const int m0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
     // 8 warps: warp w computes rows wm..wm+15 and columns wn..wn+31 of the tile.
@@ -90,33 +94,47 @@ __global__ void __launch_bounds__(256) gemm_kernel(const TA *__restrict__ A, int
     for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) acc[i][j] = 0.f;
-    for (int k0 = 0; k0 < K; k0 += 16) {
-        for (int t = tid; t < 1024; t += 256) {
-            const int mm = AT ? t % 64 : t / 16, kk = AT ? t / 64 : t % 16;
+    // Element e = tid + 256 i of a slice: A as (m, k), B as (k, n), each in
+    // the order that keeps a warp's global loads contiguous.
+    float ra[8], rb[8];
+    auto load = [&](int k0) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int e = tid + 256 * i;
+            const int mm = AT ? e % 64 : e / BK, kk = AT ? e / 64 : e % BK;
             const int gm = m0 + mm, gk = k0 + kk;
-            float v = 0.f;
-            if (gm < M && gk < K) v = to_f(AT ? A[(size_t) gk * lda + gm] : A[(size_t) gm * lda + gk]);
-            As[kk][mm] = v;
+            ra[i] = (gm < M && gk < K) ? to_f(AT ? A[(size_t) gk * lda + gm] : A[(size_t) gm * lda + gk]) : 0.f;
+            const int nn = BT ? e / BK : e % 64, kb = BT ? e % BK : e / 64;
+            const int gn = n0 + nn, gkb = k0 + kb;
+            rb[i] = (gn < N && gkb < K) ? to_f(BT ? B[(size_t) gn * ldb + gkb] : B[(size_t) gkb * ldb + gn]) : 0.f;
         }
-        for (int t = tid; t < 1024; t += 256) {
-            const int nn = BT ? t / 16 : t % 64, kk = BT ? t % 16 : t / 64;
-            const int gn = n0 + nn, gk = k0 + kk;
-            float v = 0.f;
-            if (gn < N && gk < K) v = to_f(BT ? B[(size_t) gn * ldb + gk] : B[(size_t) gk * ldb + gn]);
-            Bs[kk][nn] = v;
+    };
+    auto store = [&](int buf) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int e = tid + 256 * i;
+            As[buf][AT ? e / 64 : e % BK][AT ? e % 64 : e / BK] = ra[i];
+            Bs[buf][BT ? e % BK : e / 64][BT ? e / BK : e % 64] = rb[i];
         }
-        __syncthreads();
+    };
+    load(0);
+    store(0);
+    __syncthreads();
+    int buf = 0;
+    for (int k0 = 0; k0 < K; k0 += BK) {
+        const bool more = k0 + BK < K;
+        if (more) load(k0 + BK);  // in flight during the MMAs below
         // Tensor cores: per 8-deep k step, the warp's 16 x 32 block of C as
         // four m16n8k8 TF32 MMAs. A float32 operand is split into a TF32 high
         // part and the TF32 rounding of its remainder, and the products
         // hi*hi + hi*lo + lo*hi accumulate in float32, which keeps float32
-        // accuracy; a BF16 operand is exact in TF32 (no low part).
+        // accuracy; a BF16 operand is exact in TF32 (no low part, one MMA less).
 #pragma unroll
-        for (int kk = 0; kk < 16; kk += 8) {
+        for (int kk = 0; kk < BK; kk += 8) {
             uint32_t ah[4], al[4];
             {
-                const float av[4] = {As[kk + tq][wm + g], As[kk + tq][wm + g + 8], As[kk + tq + 4][wm + g],
-                                     As[kk + tq + 4][wm + g + 8]};
+                const float av[4] = {As[buf][kk + tq][wm + g], As[buf][kk + tq][wm + g + 8],
+                                     As[buf][kk + tq + 4][wm + g], As[buf][kk + tq + 4][wm + g + 8]};
 #pragma unroll
                 for (int i = 0; i < 4; ++i) split_tf32(av[i], ah[i], al[i]);
             }
@@ -124,14 +142,23 @@ __global__ void __launch_bounds__(256) gemm_kernel(const TA *__restrict__ A, int
             for (int nt = 0; nt < 4; ++nt) {
                 const int nb = wn + nt * 8;
                 uint32_t bh[2], bl[2];
-                split_tf32(Bs[kk + tq][nb + g], bh[0], bl[0]);
-                split_tf32(Bs[kk + tq + 4][nb + g], bh[1], bl[1]);
-                mma_tf32(acc[nt], ah, bh);
-                mma_tf32(acc[nt], ah, bl);
-                mma_tf32(acc[nt], al, bh);
+                if (kBExact) {
+                    bh[0] = __float_as_uint(Bs[buf][kk + tq][nb + g]);
+                    bh[1] = __float_as_uint(Bs[buf][kk + tq + 4][nb + g]);
+                    mma_tf32(acc[nt], ah, bh);
+                    mma_tf32(acc[nt], al, bh);
+                } else {
+                    split_tf32(Bs[buf][kk + tq][nb + g], bh[0], bl[0]);
+                    split_tf32(Bs[buf][kk + tq + 4][nb + g], bh[1], bl[1]);
+                    mma_tf32(acc[nt], ah, bh);
+                    mma_tf32(acc[nt], ah, bl);
+                    mma_tf32(acc[nt], al, bh);
+                }
             }
         }
+        if (more) store(buf ^ 1);
         __syncthreads();
+        buf ^= 1;
     }
 #pragma unroll
     for (int nt = 0; nt < 4; ++nt) {
@@ -384,7 +411,7 @@ struct Trainer {
 int check_shape(uint32_t d, uint32_t R) {
     if (d == 0 || d > 256 || d % 8) return set_error(PANNS_EINVAL, "mlp: need d a multiple of 8, 8 <= d <= 256");
     if (R == 0 || R > (uint32_t) kMlpMaxR || R % kMlpH)
-        return set_error(PANNS_EINVAL, "mlp: need R a multiple of 256, R <= 1024");
+        return set_error(PANNS_EINVAL, "mlp: need R a multiple of 256, R <= 4096");
     return PANNS_OK;
 }
 
@@ -566,25 +593,32 @@ int kmeans_run(const float *rows, uint32_t n, uint32_t d, uint32_t k, uint32_t i
     return PANNS_OK;
 }
 
-int nearest_center(const float *rows, uint32_t n, uint32_t d, const uint32_t *center_rows, uint32_t k,
-                   uint32_t *cell, cudaStream_t s) {
-    Dev<float> cent, cn, G;
-    const uint32_t chunk = std::min<uint32_t>(n, 65536);
-    LCU(cent.alloc((size_t) k * d));
+int nearest_centroid(const float *rows, uint32_t n, uint32_t d, const float *cent, uint32_t k, uint32_t *cell,
+                     cudaStream_t s) {
+    Dev<float> cn, G;
+    const uint32_t chunk = std::min<uint32_t>(n, std::max<uint32_t>(1024u, (uint32_t) std::min<uint64_t>(65536, (1ull << 29) / k)));
     LCU(cn.alloc(k));
     LCU(G.alloc((size_t) chunk * k));
-    gather_rows_kernel<<<k, 128, 0, s>>>(rows, d, center_rows, k, cent.p);
-    sqnorm_kernel<<<(k + 255) / 256, 256, 0, s>>>(cent.p, k, d, cn.p);
+    sqnorm_kernel<<<(k + 255) / 256, 256, 0, s>>>(cent, k, d, cn.p);
     LCU(cudaGetLastError());
     for (uint32_t r0 = 0; r0 < n; r0 += chunk) {
         const uint32_t rows_c = std::min(chunk, n - r0);
-        LCU((gemm<float, float, false, true>(rows + (size_t) r0 * d, d, cent.p, d, G.p, k, rows_c, k, d, nullptr, 0,
+        LCU((gemm<float, float, false, true>(rows + (size_t) r0 * d, d, cent, d, G.p, k, rows_c, k, d, nullptr, 0,
                                              s)));
         argmin_kernel<<<(rows_c * 32 + 255) / 256, 256, 0, s>>>(G.p, rows_c, k, cn.p, cell + r0);
         LCU(cudaGetLastError());
     }
     LCU(cudaStreamSynchronize(s));
     return PANNS_OK;
+}
+
+int nearest_center(const float *rows, uint32_t n, uint32_t d, const uint32_t *center_rows, uint32_t k,
+                   uint32_t *cell, cudaStream_t s) {
+    Dev<float> cent;
+    LCU(cent.alloc((size_t) k * d));
+    gather_rows_kernel<<<k, 128, 0, s>>>(rows, d, center_rows, k, cent.p);
+    LCU(cudaGetLastError());
+    return nearest_centroid(rows, n, d, cent.p, k, cell, s);
 }
 
 namespace {
@@ -634,51 +668,85 @@ __global__ void rows_from_chain_major_kernel(const float *__restrict__ q_cm, uin
     }
 }
 
-// One warp per query: the decision from its logits Z[q] (R) and its second
-// hidden layer H2[q] (256). Lane t owns logits t, t + 32, ... (R / 32 <= 32
-// of them in registers) and hidden units 8t..8t+7.
-__global__ void __launch_bounds__(256) decide_kernel(MlpDev m, const float *__restrict__ H2,
-                                                     const float *__restrict__ Z, uint32_t nq, uint32_t L,
-                                                     const uint32_t *__restrict__ Lq_in, uint32_t K,
-                                                     uint32_t *__restrict__ record) {
-    const int lane = threadIdx.x & 31;
-    const uint32_t q = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (q >= nq) return;
-    const uint32_t R = m.R, nc = R / 32;
-    // L-budget regressor.
-    const float *h = H2 + (size_t) q * kMlpH + lane * 8;
+// The regressor output r = wl . h2 + bl of one query (lane t holds hidden
+// units 8t..8t+7), reduced over the warp.
+__device__ __forceinline__ float regressor(const MlpDev &m, const float *__restrict__ h2, int lane) {
+    const float *h = h2 + lane * 8;
     float r = 0.f;
 #pragma unroll
     for (int j = 0; j < 8; ++j) r = fmaf(m.wl[lane * 8 + j], h[j], r);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
-    r += m.bl;
-    // Logits and the largest softmax probability.
-    const float *z = Z + (size_t) q * R;
-    float v[kMlpMaxR / 32];
-    float mx = PANNS_NEG_INF;
-#pragma unroll
-    for (int c = 0; c < kMlpMaxR / 32; ++c) {
-        v[c] = (uint32_t) c < nc ? z[c * 32 + lane] : PANNS_NEG_INF;
-        mx = fmaxf(mx, v[c]);
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    float se = 0.f;
-#pragma unroll
-    for (int c = 0; c < kMlpMaxR / 32; ++c)
-        if ((uint32_t) c < nc) se += expf(v[c] - mx);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) se += __shfl_xor_sync(0xffffffffu, se, o);
-    const float conf = 1.f / se;  // softmax probability of the largest logit
-    const bool fallback = !(conf >= m.min_conf);
-    const uint32_t Lc = Lq_in ? Lq_in[q] : L;
+    return r + m.bl;
+}
+
+// Queue length and fallback of one query from its confidence and regressor.
+__device__ __forceinline__ uint32_t decide_L(const MlpDev &m, float conf, float r, uint32_t Lc, uint32_t K,
+                                             bool &fallback) {
+    fallback = !(conf >= m.min_conf);
     uint32_t Lq = Lc;
     if (!fallback && m.use_L) {
         const float x = m.L_scale * expf(m.L_exp * r);
         const uint32_t lo = max(K, min(m.L_min, Lc));
         if (x < (float) Lc) Lq = max(lo, (uint32_t) ceilf(fmaxf(x, 0.f)));
     }
+    return Lq;
+}
+
+// Warp argmax of (best, bi) pairs, ties to the lower index.
+__device__ __forceinline__ void warp_argmax(float &best, uint32_t &bi) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const float b2 = __shfl_xor_sync(0xffffffffu, best, o);
+        const uint32_t i2 = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (b2 > best || (b2 == best && i2 < bi)) {
+            best = b2;
+            bi = i2;
+        }
+    }
+}
+
+// One warp per query: the decision from its logits Z[q] (R) and its second
+// hidden layer H2[q] (256). Up to 1,024 classes the logits sit in registers
+// (lane t owns logits t, t + 32, ...); beyond, they are read from Z (scratch)
+// once per pass, and chosen ones are overwritten with -inf there.
+template <bool REGS>
+__global__ void __launch_bounds__(256) decide_kernel(MlpDev m, const float *__restrict__ H2, float *__restrict__ Z,
+                                                     uint32_t nq, uint32_t L, const uint32_t *__restrict__ Lq_in,
+                                                     uint32_t K, uint32_t *__restrict__ record) {
+    constexpr int NC = REGS ? 32 : 1;  // logits per lane held in registers
+    const int lane = threadIdx.x & 31;
+    const uint32_t q = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (q >= nq) return;
+    const uint32_t R = m.R, nc = R / 32;
+    const float r = regressor(m, H2 + (size_t) q * kMlpH, lane);
+    float *z = Z + (size_t) q * R;
+    float v[NC];
+    float mx = PANNS_NEG_INF;
+    if (REGS) {
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            v[c] = (uint32_t) c < nc ? z[c * 32 + lane] : PANNS_NEG_INF;
+            mx = fmaxf(mx, v[c]);
+        }
+    } else {
+        for (uint32_t c = 0; c < nc; ++c) mx = fmaxf(mx, z[c * 32 + lane]);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    float se = 0.f;
+    if (REGS) {
+#pragma unroll
+        for (int c = 0; c < NC; ++c)
+            if ((uint32_t) c < nc) se += expf(v[c] - mx);
+    } else {
+        for (uint32_t c = 0; c < nc; ++c) se += expf(z[c * 32 + lane] - mx);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) se += __shfl_xor_sync(0xffffffffu, se, o);
+    const float conf = 1.f / se;  // softmax probability of the largest logit
+    bool fallback;
+    const uint32_t Lq = decide_L(m, conf, r, Lq_in ? Lq_in[q] : L, K, fallback);
     uint32_t *rec = record + (size_t) q * kMlpRecWords;
     uint32_t E = 0;
     if (!fallback && m.use_entry) {
@@ -687,28 +755,35 @@ __global__ void __launch_bounds__(256) decide_kernel(MlpDev m, const float *__re
         for (; E < want; ++E) {
             float best = PANNS_NEG_INF;
             uint32_t bi = 0xffffffffu;
+            if (REGS) {
 #pragma unroll
-            for (int c = 0; c < kMlpMaxR / 32; ++c)
-                if (v[c] > best) {
-                    best = v[c];
-                    bi = c * 32 + lane;
-                }
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                const float b2 = __shfl_xor_sync(0xffffffffu, best, o);
-                const uint32_t i2 = __shfl_xor_sync(0xffffffffu, bi, o);
-                if (b2 > best || (b2 == best && i2 < bi)) {
-                    best = b2;
-                    bi = i2;
+                for (int c = 0; c < NC; ++c)
+                    if (v[c] > best) {
+                        best = v[c];
+                        bi = c * 32 + lane;
+                    }
+            } else {
+                for (uint32_t c = 0; c < nc; ++c) {
+                    const float x = z[c * 32 + lane];
+                    if (x > best) {
+                        best = x;
+                        bi = c * 32 + lane;
+                    }
                 }
             }
+            warp_argmax(best, bi);
             if (bi >= R) break;  // only -inf or NaN left
             if (lane == 0) rec[2 + E] = __ldg(m.rep + bi);
             if (lane == (int) (bi & 31)) {
+                if (REGS) {
 #pragma unroll
-                for (int c = 0; c < kMlpMaxR / 32; ++c)
-                    if ((uint32_t) c == (bi >> 5)) v[c] = PANNS_NEG_INF;
+                    for (int c = 0; c < NC; ++c)
+                        if ((uint32_t) c == (bi >> 5)) v[c] = PANNS_NEG_INF;
+                } else {
+                    z[bi] = PANNS_NEG_INF;
+                }
             }
+            __syncwarp();
         }
     }
     if (lane == 0) {
@@ -735,8 +810,12 @@ cudaError_t mlp_decide(const MlpDev &m, const float *q_cm, uint32_t dpad, uint32
         if (e == cudaSuccess)
             e = gemm<float, __nv_bfloat16, false, false>(w.H2, H, m.w3, R, w.Z, R, (int) rows, R, H, m.b3, 0, s);
         if (e == cudaSuccess) {
-            decide_kernel<<<(rows + 7) / 8, 256, 0, s>>>(m, w.H2, w.Z, rows, L, Lq ? Lq + r0 : nullptr, K,
-                                                         record + (size_t) r0 * kMlpRecWords);
+            if (m.R <= 1024)
+                decide_kernel<true><<<(rows + 7) / 8, 256, 0, s>>>(m, w.H2, w.Z, rows, L, Lq ? Lq + r0 : nullptr, K,
+                                                                   record + (size_t) r0 * kMlpRecWords);
+            else
+                decide_kernel<false><<<(rows + 7) / 8, 256, 0, s>>>(m, w.H2, w.Z, rows, L, Lq ? Lq + r0 : nullptr, K,
+                                                                    record + (size_t) r0 * kMlpRecWords);
             e = cudaGetLastError();
         }
     }

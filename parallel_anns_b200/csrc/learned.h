@@ -30,6 +30,10 @@ int kmeans_run(const float *rows, uint32_t n, uint32_t d, uint32_t k, uint32_t i
 int nearest_center(const float *rows, uint32_t n, uint32_t d, const uint32_t *center_rows, uint32_t k,
                    uint32_t *cell, cudaStream_t stream);
 
+// The same with the k centres given as rows of width d (device, k x d).
+int nearest_centroid(const float *rows, uint32_t n, uint32_t d, const float *centroids, uint32_t k, uint32_t *cell,
+                     cudaStream_t stream);
+
 // Packs the float32 training parameters (layout of panns_mlp_param_count)
 // into the inference layout read by mlp_decide: BF16 w1 (d x 256),
 // w2 (256 x 256), w3 (256 x R) into `wbf` (device, 256 (d + 256 + R)

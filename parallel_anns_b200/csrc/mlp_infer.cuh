@@ -27,7 +27,7 @@
 namespace panns {
 
 constexpr int kMlpH = 256;      // hidden width
-constexpr int kMlpMaxR = 1024;  // entry classes (multiple of 256)
+constexpr int kMlpMaxR = 4096;  // entry classes (multiple of 256)
 constexpr int kMlpMaxE = 64;    // learned entries per query (WarpMem::cand holds them)
 constexpr int kMlpRecWords = 2 + kMlpMaxE;  // per-query record: L_q | fallback << 31, E, entries
 #define PANNS_NEG_INF __int_as_float(0xff800000u)

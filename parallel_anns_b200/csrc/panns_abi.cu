@@ -661,9 +661,8 @@ int check_params(panns_index *h, const panns_search_params *p) {
             return fail(PANNS_EINVAL, "search: warps_per_query must be 0, 1, 2, 4 or 8");
         const bool ok = p->mode == PANNS_MODE_NSG_SEQ || p->mode == PANNS_MODE_TOP_M ||
                         (p->mode == PANNS_MODE_PSS_V5 && p->T == 1);
-        if (!ok || (p->flags & PANNS_FLAG_LEARNED))
-            return fail(PANNS_EINVAL, "search: warps_per_query > 1 is for NSG_SEQ, TOP_M and PSS_V5 at T = 1, "
-                                      "without PANNS_FLAG_LEARNED");
+        if (!ok)
+            return fail(PANNS_EINVAL, "search: warps_per_query > 1 is for NSG_SEQ, TOP_M and PSS_V5 at T = 1");
         if (h->max_deg > (uint32_t) kBuf)
             return fail(PANNS_EINVAL, "search: warps_per_query > 1 needs a graph degree <= " + std::to_string(kBuf));
     }
@@ -801,7 +800,7 @@ static int launch_search(panns_index *h, const panns_search_params *p, float *d_
     uint32_t wpq = p->warps_per_query > 1 ? p->warps_per_query : 1u;
     if (p->warps_per_query == 0 && p->warps_per_block == 0 && p->blocks_per_sm == 0 &&
         (p->mode == PANNS_MODE_NSG_SEQ || p->mode == PANNS_MODE_TOP_M || (p->mode == PANNS_MODE_PSS_V5 && p->T == 1)) &&
-        !(p->flags & PANNS_FLAG_LEARNED) && h->max_deg <= (uint32_t) kBuf) {
+        h->max_deg <= (uint32_t) kBuf) {
         // Automatic block shape (same ids either way), from the 1M x 96 and
         // 1M x 128 measurements: 8 warps per query up to one query per SM and
         // for queues of 2048 and more, 2 up to ten queries per SM, else one.
@@ -1520,7 +1519,7 @@ extern "C" int panns_set_learned(panns_index *h, const float *params, uint32_t R
     int rc = finalize(h);
     if (rc) return rc;
     if (R == 0 || R > (uint32_t) kMlpMaxR || R % kMlpH)
-        return fail(PANNS_EINVAL, "panns_set_learned: need R a multiple of 256, R <= 1024");
+        return fail(PANNS_EINVAL, "panns_set_learned: need R a multiple of 256, R <= 4096");
     if (lp->E > (uint32_t) kMlpMaxE) return fail(PANNS_EINVAL, "panns_set_learned: need E <= 64");
     if (!(lp->min_conf >= 0.f && lp->min_conf <= 1.f))
         return fail(PANNS_EINVAL, "panns_set_learned: need 0 <= min_conf <= 1");

@@ -58,6 +58,35 @@ def gaussian_mixture(n: int, d: int, n_components: int = 64, sigma: float = 0.3,
     return np.ascontiguousarray(x, dtype=np.float32)
 
 
+@torch.no_grad()
+def gaussian_mixture_gpu(n: int, d: int, n_components: int = 4096, sigma: float = 0.3, seed: int = 0,
+                         means_seed: int | None = None, chunk: int = 1 << 20, device: int = 0) -> np.ndarray:
+    """``n`` float32 vectors from the same kind of mixture as ``gaussian_mixture``
+    (means ~ N(0, 1), per-coordinate sigma, unit norm), drawn on the GPU with
+    torch's seeded Philox generator, chunk by chunk into host memory, for
+    bases too large for host-side float64 temporaries (100M x 96). The means
+    come from ``means_seed`` (default ``seed``); chunk i uses the stream of
+    (seed, i), so the result does not depend on memory size."""
+    dev = torch.device("cuda", device)
+    gm = torch.Generator(device=dev)
+    gm.manual_seed(seed if means_seed is None else means_seed)
+    means = torch.randn((n_components, d), generator=gm, device=dev, dtype=torch.float32)
+    out = np.empty((n, d), dtype=np.float32)
+    pinned = torch.empty((min(chunk, n), d), dtype=torch.float32).pin_memory()
+    g = torch.Generator(device=dev)
+    for i, r0 in enumerate(range(0, n, chunk)):
+        m = min(chunk, n - r0)
+        g.manual_seed((seed * 1_000_003 + i) & 0x7FFFFFFFFFFFFFFF)
+        comp = torch.randint(0, n_components, (m,), generator=g, device=dev)
+        x = torch.randn((m, d), generator=g, device=dev, dtype=torch.float32) * sigma + means[comp]
+        nrm = torch.linalg.vector_norm(x.double(), dim=1, keepdim=True)
+        nrm[nrm == 0] = 1.0
+        x = (x.double() / nrm).float()
+        pinned[:m].copy_(x)
+        out[r0:r0 + m] = pinned[:m].numpy()
+    return out
+
+
 def uint8_cube(n: int, d: int = 128, seed: int = 0) -> np.ndarray:
     """Integer-valued components uniform in 0..255, stored as uint8 then cast."""
     rng = np.random.default_rng(seed)

@@ -32,7 +32,8 @@ EXPORTS = [
     "panns_mlp_param_count", "panns_mlp_loss_grad", "panns_mlp_forward", "panns_mlp_train",
     "panns_kmeans", "panns_set_learned", "panns_learned_record",
     # include/panns_build.h
-    "panns_build_nsg", "panns_build_nsg_ex", "panns_graph_info", "panns_graph_copy", "panns_graph_save_nsg", "panns_graph_free",
+    "panns_build_nsg", "panns_build_nsg_ex", "panns_build_nsg_cells", "panns_graph_cells", "panns_graph_info",
+    "panns_graph_copy", "panns_graph_save_nsg", "panns_graph_free",
     "panns_efanna_build",
 ]
 
@@ -128,6 +129,8 @@ def load(build_if_missing: bool = True):
     L.panns_learned_record.argtypes = [P, u32, P]
     L.panns_build_nsg.argtypes = [i32, P, u32, u32, u32, u32, ctypes.POINTER(P)]
     L.panns_build_nsg_ex.argtypes = [i32, P, u32, u32, u32, u32, u32, ctypes.POINTER(P)]
+    L.panns_build_nsg_cells.argtypes = [i32, P, u32, u32, u32, u32, u32, u32, u32, u32, u32, u32, ctypes.POINTER(P)]
+    L.panns_graph_cells.argtypes = [P, P, P, P, P]
     L.panns_graph_info.argtypes = [P, P, P, P, P, P]
     L.panns_graph_copy.argtypes = [P, P, P, P]
     L.panns_graph_save_nsg.argtypes = [P, ctypes.c_char_p]

@@ -46,8 +46,22 @@ def spec_mixture_10m_d96(n=10_000_000, nq=10_000):
             "gt_k": 100}
 
 
+def spec_mixture_100m_d96(n=100_000_000, nq=10_000):
+    """The large uneven-batch config: N = 100M, d = 96 from a 4,096-component
+    mixture (drawn on the GPU), R = 48; graph from exact 64-NN within each of
+    10,000 k-means cells and its 3 nearest cells, RNG-pruned to R, reverse
+    edges up to R (the mixture's components are tight and far apart, and
+    without them a component falls into fragments that only the entry's
+    repair links join), medoid entry, repair. Held in memory (no files):
+    at this size the reference's loaders would need the whole index twice
+    over in host memory."""
+    return {"name": f"mixture4096_n{n}_d96_q{nq}_R48", "n": n, "d": 96, "nq": nq, "R": 48, "knn_k": 64,
+            "components": 4096, "sigma": 0.3, "base_seed": 1004, "query_seed": 2004, "gt_k": 100,
+            "cells": max(1, min(10_000, n // 1000)), "probe": 3, "reverse": True, "reps": 4096, "large": True}
+
+
 SPECS = {"mixture_1m_d96": spec_batched_fp32_1m, "u8_1m_d128": spec_u8_1m_d128,
-         "mixture_10m_d96": spec_mixture_10m_d96}
+         "mixture_10m_d96": spec_mixture_10m_d96, "mixture_100m_d96": spec_mixture_100m_d96}
 
 
 def describe(spec) -> str:
@@ -65,6 +79,9 @@ def vectors(spec, count, seed):
     mixture means)."""
     if spec.get("kind") == "uint8":
         return ds.uint8_cube(count, spec["d"], seed=seed)
+    if spec.get("large"):
+        return ds.gaussian_mixture_gpu(count, spec["d"], spec["components"], spec["sigma"], seed=seed,
+                                       means_seed=spec["base_seed"])
     return ds.gaussian_mixture(count, spec["d"], spec["components"], spec["sigma"], seed=seed,
                                means_seed=spec["base_seed"])
 
@@ -126,8 +143,12 @@ def build_graph(base, spec, device=None):
     when a GPU is present, else the torch restatement in datasets.py (same rule)."""
     import torch
     if torch.cuda.is_available():
-        from .graph import build_nsg
+        from .graph import build_nsg, build_nsg_cells
         dev = torch.device(device) if device is not None else torch.device("cuda", 0)
+        if spec.get("cells"):
+            return build_nsg_cells(base, R=spec["R"], knn_k=spec["knn_k"], cells=spec["cells"], probe=spec["probe"],
+                                   sample=min(spec["n"], 2_000_000), iters=10, seed=1, device=dev.index or 0,
+                                   reverse=spec.get("reverse", False))
         return build_nsg(base, R=spec["R"], knn_k=spec["knn_k"], device=dev.index or 0)
     return ds.build_nsg_graph(base, R=spec["R"], knn_k=spec["knn_k"], device="cpu")
 

@@ -127,6 +127,11 @@ def check_learned_search(ix, base, q, g, model, K, L, M, lp):
     bad = np.nonzero((ids != ref).any(1))[0]
     assert bad.size == 0, bad[:10]
     assert st["n_dist"] == nd
+    # several warps per query from the same decisions: the same ids and counts
+    for wq in (2, 4):
+        ids_w, st_w = ix.search(K=K, L=L, mode=N.MODE_TOP_M if M > 1 else N.MODE_NSG_SEQ, M=M, flags=N.FLAG_LEARNED,
+                                warps_per_query=wq)
+        assert np.array_equal(ids_w, ids) and st_w["n_dist"] == nd, wq
     return ids, Lq, fb
 
 
@@ -142,6 +147,19 @@ def test_learned_search_exact_given_decisions(small):
                   (dict(E=8, L_init=24, use_L=True, L_scale=0.8, L_exp=0.6, L_min=64), 1),
                   (dict(E=40, L_init=0, use_L=False), 8)):
         check_learned_search(ix, base, q, g, model, 50, 200, M, lp)
+
+
+def test_learned_search_exact_given_decisions_many_classes(small):
+    """More entry classes than the batched inference keeps in registers
+    (R = 2,048: the logits are read from its scratch)."""
+    from parallel_anns_b200 import learned as LE
+    ix, base, q, g = small
+    rng = np.random.default_rng(7)
+    reps = rng.choice(base.shape[0], 2048, replace=False).astype(np.uint32)
+    p = LE.init_params(96, 2048, seed=11, y_mean=np.log(150.0))
+    p[-2049:] += rng.normal(0, 0.5, 2049).astype(np.float32)  # spread logits and the L output
+    model = LE.LearnedModel(96, 2048, p, reps)
+    check_learned_search(ix, base, q, g, model, 50, 200, 4, dict(E=16, L_init=8, use_L=True, L_scale=1.0))
 
 
 def test_unconfident_network_runs_plain_search(small):
