@@ -51,8 +51,8 @@ int panns_build_nsg_ex(int device, const float *base, uint32_t n, uint32_t d, ui
 
 /* The construction of the large-graph configuration (100M vectors on one GPU,
  * where all pairs are out of reach): the vertices are partitioned into
- * `cells` k-means cells (Lloyd, `iters` rounds from `cells` distinct rows
- * chosen by `seed`, on `sample` rows taken at a fixed stride; then every
+ * `cells` k-means cells (Lloyd, `iters` rounds from a farthest-point start
+ * seeded by `seed`, on `sample` rows taken at a fixed stride; then every
  * vertex goes to its nearest centroid), and the k-NN list of vertex a holds
  * the knn_k vertices b != a with the smallest (d64(a, b), b) among the
  * members of a's cell and of the `probe` cells whose centroids are nearest to

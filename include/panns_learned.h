@@ -64,8 +64,8 @@ typedef struct {
 int panns_mlp_train(int device, const panns_mlp_train_params *tp, const float *X, const uint16_t *cells,
                     const float *y, uint32_t n, float *params, double *epoch_loss);
 
-/* k-means over the handle's base vectors (Lloyd, `iters` rounds, k distinct
- * rows as the seeded start). Outputs (host, each optional): rep_ids k original
+/* k-means over the handle's base vectors (Lloyd, `iters` rounds from a
+ * farthest-point start, its first centre chosen by `seed`). Outputs (host, each optional): rep_ids k original
  * ids, the base vertex of each cell nearest its centroid; assign n cells per
  * original id; centroids k x d. */
 int panns_kmeans(panns_index *h, uint32_t k, uint32_t iters, uint32_t seed, uint32_t *rep_ids,

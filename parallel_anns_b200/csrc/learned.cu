@@ -430,6 +430,65 @@ __global__ void gather_rows_kernel(const float *__restrict__ rows, uint32_t d, c
     for (uint32_t j = threadIdx.x; j < d; j += blockDim.x) out[(size_t) c * d + j] = rows[(size_t) idx[c] * d + j];
 }
 
+// Farthest-point seeding, all on the GPU. mind[s] = the squared distance of
+// sample row sidx[s] to the nearest centre chosen so far; kpp_update folds
+// in the newest centre (sample slot *slot).
+__global__ void kpp_update_kernel(const float *__restrict__ rows, uint32_t d, const uint32_t *__restrict__ sidx,
+                                  uint32_t S, const uint32_t *__restrict__ slot, float *__restrict__ mind) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= S) return;
+    const float *x = rows + (size_t) sidx[t] * d;
+    const float *c = rows + (size_t) sidx[*slot] * d;
+    float acc = 0.f;
+    for (uint32_t j = 0; j < d; ++j) {
+        const float u = x[j] - c[j];
+        acc = fmaf(u, u, acc);
+    }
+    mind[t] = fminf(mind[t], acc);
+}
+
+// One block of 1024 threads: the next centre, the sample slot with the
+// largest mind (ties to the lower slot).
+__global__ void __launch_bounds__(1024) kpp_pick_kernel(const float *__restrict__ mind, uint32_t S,
+                                                        uint32_t *__restrict__ slot) {
+    __shared__ float bv[32];
+    __shared__ uint32_t bi[32];
+    float best = -1.f;
+    uint32_t bidx = 0xffffffffu;
+    for (uint32_t i = threadIdx.x; i < S; i += blockDim.x)
+        if (mind[i] > best) {  // ascending i: the lower slot wins ties
+            best = mind[i];
+            bidx = i;
+        }
+    for (int o = 16; o > 0; o >>= 1) {
+        const float v2 = __shfl_xor_sync(0xffffffffu, best, o);
+        const uint32_t i2 = __shfl_xor_sync(0xffffffffu, bidx, o);
+        if (v2 > best || (v2 == best && i2 < bidx)) {
+            best = v2;
+            bidx = i2;
+        }
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) {
+        bv[w] = best;
+        bi[w] = bidx;
+    }
+    __syncthreads();
+    if (w == 0) {
+        best = bv[l];
+        bidx = bi[l];
+        for (int o = 16; o > 0; o >>= 1) {
+            const float v2 = __shfl_xor_sync(0xffffffffu, best, o);
+            const uint32_t i2 = __shfl_xor_sync(0xffffffffu, bidx, o);
+            if (v2 > best || (v2 == best && i2 < bidx)) {
+                best = v2;
+                bidx = i2;
+            }
+        }
+        if (l == 0) *slot = bidx < S ? bidx : 0u;
+    }
+}
+
 __global__ void sqnorm_kernel(const float *__restrict__ rows, uint32_t n, uint32_t d, float *__restrict__ out) {
     const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= n) return;
@@ -519,17 +578,34 @@ __global__ void cell_kernel(const float *__restrict__ rows, uint32_t d, const ui
 int kmeans_run(const float *rows, uint32_t n, uint32_t d, uint32_t k, uint32_t iters, uint32_t seed,
                float *cent, uint32_t *assign, uint32_t *rep, cudaStream_t s) {
     if (k == 0 || k > n) return set_error(PANNS_EINVAL, "kmeans: need 0 < k <= N");
-    // Start: k distinct rows in a seeded order.
+    // Start: farthest-point seeding (Gonzalez, 1985) on S rows at a fixed
+    // stride: a seeded first centre, then each next one the sample row
+    // farthest from the centres so far (on the GPU). Far-apart clusters then
+    // each get a centre before any is split, which random starts (and D^2
+    // sampling, with as many centres as clusters) miss.
     std::vector<uint32_t> start(k);
     {
+        const uint32_t S = (uint32_t) std::min<uint64_t>(n, std::max<uint64_t>(k, 32ull * k));
+        std::vector<uint32_t> sidx(S), slots(k);
+        for (uint32_t i = 0; i < S; ++i) sidx[i] = (uint32_t) ((uint64_t) i * n / S);
         std::mt19937_64 rng(seed);
-        std::vector<uint8_t> used(n, 0);
-        for (uint32_t c = 0; c < k;) {
-            const uint32_t r = (uint32_t) (rng() % n);
-            if (used[r]) continue;
-            used[r] = 1;
-            start[c++] = r;
+        Dev<uint32_t> dsidx, dslot;
+        Dev<float> mind;
+        LCU(dsidx.alloc(S));
+        LCU(dslot.alloc(k));
+        LCU(mind.alloc(S));
+        LCU(cudaMemcpyAsync(dsidx.p, sidx.data(), S * 4ull, cudaMemcpyHostToDevice, s));
+        LCU(cudaMemsetAsync(mind.p, 0x7f, S * 4ull, s));  // 3.4e38: larger than any distance
+        const uint32_t first = (uint32_t) (rng() % S);
+        LCU(cudaMemcpyAsync(dslot.p, &first, 4, cudaMemcpyHostToDevice, s));
+        for (uint32_t c = 0; c < k; ++c) {
+            kpp_update_kernel<<<(S + 255) / 256, 256, 0, s>>>(rows, d, dsidx.p, S, dslot.p + c, mind.p);
+            if (c + 1 < k) kpp_pick_kernel<<<1, 1024, 0, s>>>(mind.p, S, dslot.p + c + 1);
         }
+        LCU(cudaGetLastError());
+        LCU(cudaMemcpyAsync(slots.data(), dslot.p, k * 4ull, cudaMemcpyDeviceToHost, s));
+        LCU(cudaStreamSynchronize(s));
+        for (uint32_t c = 0; c < k; ++c) start[c] = sidx[slots[c]];
     }
     Dev<uint32_t> didx, doff, dmem;
     Dev<float> cn, G;

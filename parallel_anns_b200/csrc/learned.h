@@ -16,7 +16,8 @@ namespace panns {
 int set_error(int code, const std::string &msg);
 
 // Lloyd's k-means on n row-major float32 rows of width d (device), k
-// centroids initialised from k distinct rows chosen by `seed`. On return
+// centroids initialised by farthest-point seeding (the first centre chosen
+// by `seed`) on up to 32 k rows at a fixed stride. On return
 // (enqueued on `stream`, synchronised): centroids (k x d, device), assign[i]
 // = cell of row i (device), rep[c] = the row of cell c nearest to its
 // centroid (device; cells left empty get a row no other cell uses).
