@@ -1183,12 +1183,14 @@ int panns_ground_truth(panns_index *h, const float *queries, uint32_t nq, uint32
     if (rc) return rc;
     if (k == 0 || k > h->n) return fail(PANNS_EINVAL, "panns_ground_truth: need 0 < k <= N");
     CU(cudaSetDevice(h->device));
-    // 1. An upper bound per query: a top-M search for k results (exact FP32).
+    // 1. An upper bound per query: a top-M search for k results (exact FP32),
+    // with a queue that also holds every neighbour of the entry (the PANNS
+    // init list), so graphs whose parts meet only at the entry are covered.
     panns_search_params p{};
     p.mode = PANNS_MODE_TOP_M;
     p.distance = PANNS_DIST_L2;
     p.K = k;
-    p.L = std::min(h->n, std::max(2 * k, 256u));
+    p.L = std::min(h->n, std::max(std::max(2 * k, 256u), std::min(h->max_deg + 2 * k, 8192u)));
     p.M = 8;
     p.T = 1;
     p.X = 1;
@@ -1206,46 +1208,105 @@ int panns_ground_truth(panns_index *h, const float *queries, uint32_t nq, uint32
     CU(cudaMemcpyAsync(dids.p, sids.data(), (size_t) nq * k * 4, cudaMemcpyHostToDevice, h->stream));
     gt_tau_kernel<<<(nq + 3) / 4, 128, 0, h->stream>>>(h->base_raw.p, (int) h->d, dq.p, nq, dids.p, k, dtau.p);
     CU(cudaGetLastError());
-    // 2. Collect every vertex within the bound; grow the lists if any overflowed.
-    uint32_t cap = std::max(4 * k, 64u);
-    std::vector<uint32_t> cnt(nq);
-    DevBuf<double> cd;
-    DevBuf<uint32_t> ci;
-    for (int attempt = 0; attempt < 2; ++attempt) {
-        CU(cd.ensure((size_t) nq * cap));
-        CU(ci.ensure((size_t) nq * cap));
-        CU(cudaMemsetAsync(dcnt.p, 0, nq * 4ull, h->stream));
-        const uint32_t vt = (h->n + kGtV - 1) / kGtV;
-        for (uint32_t t0 = 0; t0 < vt; t0 += 65535u) {
-            dim3 grid((nq + kGtQ - 1) / kGtQ, std::min(65535u, vt - t0));
-            gt_collect_kernel<<<grid, 256, 0, h->stream>>>(h->base_raw.p, h->n, (int) h->d, dq.p, nq, dtau.p, cap,
-                                                           dcnt.p, cd.p, ci.p, t0);
+    // 2. Collect every vertex within the bound. A pass scans all vertices for
+    // a set of queries with lists of `cap` entries (counts go on past cap).
+    const uint32_t vt = (h->n + kGtV - 1) / kGtV;
+    auto collect = [&](const float *qrows, const double *tau, uint32_t m, uint32_t cap, uint32_t *dc, double *cd,
+                       uint32_t *ci) -> cudaError_t {
+        cudaError_t e = cudaMemsetAsync(dc, 0, m * 4ull, h->stream);
+        for (uint32_t t0 = 0; e == cudaSuccess && t0 < vt; t0 += 65535u) {
+            dim3 grid((m + kGtQ - 1) / kGtQ, std::min(65535u, vt - t0));
+            gt_collect_kernel<<<grid, 256, 0, h->stream>>>(h->base_raw.p, h->n, (int) h->d, qrows, m, tau, cap, dc,
+                                                           cd, ci, t0);
+            e = cudaGetLastError();
         }
-        CU(cudaGetLastError());
-        CU(cudaMemcpyAsync(cnt.data(), dcnt.p, nq * 4ull, cudaMemcpyDeviceToHost, h->stream));
-        CU(cudaStreamSynchronize(h->stream));
-        const uint32_t mx = *std::max_element(cnt.begin(), cnt.end());
-        if (mx <= cap) break;
-        if (attempt == 1) return fail(PANNS_EDEVICE, "panns_ground_truth: candidate lists overflowed twice");
-        cap = mx;
-    }
-    // 3. Exact (distance, id) order of each list; the first k are the answer.
-    std::vector<double> hd((size_t) nq * cap);
-    std::vector<uint32_t> hi((size_t) nq * cap);
-    CU(cudaMemcpyAsync(hd.data(), cd.p, hd.size() * 8, cudaMemcpyDeviceToHost, h->stream));
-    CU(cudaMemcpyAsync(hi.data(), ci.p, hi.size() * 4, cudaMemcpyDeviceToHost, h->stream));
-    CU(cudaStreamSynchronize(h->stream));
+        return e;
+    };
+    // The exact (distance, id) order of one query's list; the first k are the answer.
     std::vector<std::pair<double, uint32_t>> tmp;
-    for (uint32_t q = 0; q < nq; ++q) {
-        const uint32_t c = cnt[q];
+    auto finish = [&](uint32_t q, const double *ld, const uint32_t *li, uint32_t c) -> int {
         if (c < k) return fail(PANNS_EDEVICE, "panns_ground_truth: fewer candidates than k");
         tmp.resize(c);
-        for (uint32_t i = 0; i < c; ++i) tmp[i] = {hd[(size_t) q * cap + i], hi[(size_t) q * cap + i]};
+        for (uint32_t i = 0; i < c; ++i) tmp[i] = {ld[i], li[i]};
         std::partial_sort(tmp.begin(), tmp.begin() + k, tmp.end());
         for (uint32_t i = 0; i < k; ++i) {
             out_ids[(size_t) q * k + i] = tmp[i].second;
             if (out_dist) out_dist[(size_t) q * k + i] = tmp[i].first;
         }
+        return PANNS_OK;
+    };
+    const uint32_t cap = std::max(4 * k, 64u);
+    std::vector<uint32_t> cnt(nq);
+    std::vector<uint32_t> over;  // queries whose lists overflowed
+    {
+        DevBuf<double> cd;
+        DevBuf<uint32_t> ci;
+        CU(cd.ensure((size_t) nq * cap));
+        CU(ci.ensure((size_t) nq * cap));
+        CU(collect(dq.p, dtau.p, nq, cap, dcnt.p, cd.p, ci.p));
+        CU(cudaMemcpyAsync(cnt.data(), dcnt.p, nq * 4ull, cudaMemcpyDeviceToHost, h->stream));
+        std::vector<double> hd((size_t) nq * cap);
+        std::vector<uint32_t> hi((size_t) nq * cap);
+        CU(cudaMemcpyAsync(hd.data(), cd.p, hd.size() * 8, cudaMemcpyDeviceToHost, h->stream));
+        CU(cudaMemcpyAsync(hi.data(), ci.p, hi.size() * 4, cudaMemcpyDeviceToHost, h->stream));
+        CU(cudaStreamSynchronize(h->stream));
+        for (uint32_t q = 0; q < nq; ++q) {
+            if (cnt[q] > cap) {
+                over.push_back(q);
+                continue;
+            }
+            rc = finish(q, hd.data() + (size_t) q * cap, hi.data() + (size_t) q * cap, cnt[q]);
+            if (rc) return rc;
+        }
+    }
+    // 3. Queries whose bound was loose (the search missed their part of the
+    // graph): again, a few at a time, each list as long as its count, within
+    // 4 GiB of lists per pass.
+    const size_t budget = 4ull << 30;
+    for (size_t g0 = 0; g0 < over.size();) {
+        size_t g1 = g0;
+        uint32_t gcap = 0;
+        while (g1 < over.size()) {
+            const uint32_t c2 = std::max(gcap, cnt[over[g1]]);
+            if (g1 > g0 && (size_t) (g1 - g0 + 1) * c2 * 12 > budget) break;
+            gcap = c2;
+            ++g1;
+        }
+        const uint32_t m = (uint32_t) (g1 - g0);
+        if ((size_t) m * gcap * 12 > budget)
+            return fail(PANNS_ENOMEM, "panns_ground_truth: a query's bound holds " + std::to_string(gcap) +
+                                          " vertices, more than the 4 GiB of candidate lists allowed");
+        std::vector<float> qh((size_t) m * h->d);
+        std::vector<double> th(m);
+        for (uint32_t i = 0; i < m; ++i) {
+            const uint32_t q = over[g0 + i];
+            std::copy(queries + (size_t) q * h->d, queries + (size_t) (q + 1) * h->d, qh.begin() + (size_t) i * h->d);
+        }
+        DevBuf<float> gq;
+        DevBuf<double> gt, cd;
+        DevBuf<uint32_t> gc, ci;
+        CU(gq.ensure(qh.size()));
+        CU(gt.ensure(m));
+        CU(gc.ensure(m));
+        CU(cd.ensure((size_t) m * gcap));
+        CU(ci.ensure((size_t) m * gcap));
+        CU(cudaMemcpyAsync(gq.p, qh.data(), qh.size() * 4, cudaMemcpyHostToDevice, h->stream));
+        for (uint32_t i = 0; i < m; ++i)
+            CU(cudaMemcpyAsync(gt.p + i, dtau.p + over[g0 + i], 8, cudaMemcpyDeviceToDevice, h->stream));
+        CU(collect(gq.p, gt.p, m, gcap, gc.p, cd.p, ci.p));
+        std::vector<uint32_t> c2(m);
+        std::vector<double> hd((size_t) m * gcap);
+        std::vector<uint32_t> hi((size_t) m * gcap);
+        CU(cudaMemcpyAsync(c2.data(), gc.p, m * 4ull, cudaMemcpyDeviceToHost, h->stream));
+        CU(cudaMemcpyAsync(hd.data(), cd.p, hd.size() * 8, cudaMemcpyDeviceToHost, h->stream));
+        CU(cudaMemcpyAsync(hi.data(), ci.p, hi.size() * 4, cudaMemcpyDeviceToHost, h->stream));
+        CU(cudaStreamSynchronize(h->stream));
+        for (uint32_t i = 0; i < m; ++i) {
+            if (c2[i] > gcap) return fail(PANNS_EDEVICE, "panns_ground_truth: candidate count changed between passes");
+            rc = finish(over[g0 + i], hd.data() + (size_t) i * gcap, hi.data() + (size_t) i * gcap, c2[i]);
+            if (rc) return rc;
+        }
+        g0 = g1;
     }
     return PANNS_OK;
 }
