@@ -45,6 +45,10 @@ sys.path.insert(0, ROOT)
 METRIC = "QPS at recall@100>=0.95, 1M x 96d; learned+BF16 vs plain FP32 GPU vs CPU"
 UNIT = "queries/s"
 RECALL_TARGET = 0.95
+# Operating points are tuned on held-out queries to the target plus a margin
+# (about three standard errors of a 10,000-query recall estimate), so that the
+# evaluated queries meet the target too.
+TUNE_TARGET = RECALL_TARGET + 0.002
 L_SWEEP = [100, 128, 160, 200, 256, 320, 400, 512, 640, 800]
 M_SWEEP = [1, 2, 4, 8, 16]
 
@@ -329,13 +333,13 @@ def bench_ours(args):
         choices = {"plain": dict(c, storage=0, learned=None), "head": c, "tables": []}
     elif rank == 0:
         t0 = time.time()
-        plain = AT.tune(handles[N.STORE_FP32], tune_q, tune_gt, K=K, target=RECALL_TARGET,
+        plain = AT.tune(handles[N.STORE_FP32], tune_q, tune_gt, K=K, target=TUNE_TARGET,
                         storages=(N.STORE_FP32,), Ms=Ms, wpbs=(2, 4), wpqs=(1, 2, 4, 8))
         cands = [plain]
         for store in stores:
             if store == N.STORE_FP32 and model is None:
                 continue
-            c = AT.tune(handles[store], tune_q, tune_gt, K=K, target=RECALL_TARGET, storages=(store,), Ms=Ms,
+            c = AT.tune(handles[store], tune_q, tune_gt, K=K, target=TUNE_TARGET, storages=(store,), Ms=Ms,
                         wpbs=(2, 4), learned_model=model, learned_opts=learned_opts if model is not None else (),
                         include_plain=store != N.STORE_FP32)
             cands.append(c)
@@ -607,9 +611,9 @@ def bench_large(args, spec):
     learned_opts = [dict(E=8, L_init=8, use_L=False), dict(E=16, L_init=16, use_L=False, min_conf=0.5)]
     t0 = time.time()
     Ms = [args.M] if args.M else M_SWEEP
-    plain = AT.tune(ix, tune_q, tune_gt, K=K, target=RECALL_TARGET, storages=(N.STORE_FP32,), Ms=Ms, wpbs=(2, 4),
+    plain = AT.tune(ix, tune_q, tune_gt, K=K, target=TUNE_TARGET, storages=(N.STORE_FP32,), Ms=Ms, wpbs=(2, 4),
                     log=log)
-    head = AT.tune(ix, tune_q, tune_gt, K=K, target=RECALL_TARGET, storages=(N.STORE_BF16,), Ms=Ms, wpbs=(2, 4),
+    head = AT.tune(ix, tune_q, tune_gt, K=K, target=TUNE_TARGET, storages=(N.STORE_BF16,), Ms=Ms, wpbs=(2, 4),
                    learned_model=model, learned_opts=learned_opts if model is not None else (), log=log)
     tm["autotune_s"] = round(time.time() - t0, 1)
     if plain.kernel_ms < head.kernel_ms:
