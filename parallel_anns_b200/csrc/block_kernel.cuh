@@ -206,94 +206,77 @@ __device__ void block_search_one(const SearchArgs &a, uint32_t q, uint8_t *smem,
         if (lane == 0) ctl[BC_SEG + w] = cnt;
     };
 
-    // The initial queue and every step's rounds go through one loop, so the
-    // block holds one inlined copy of finish_list and block_merge: a pass is
-    // an init pass (the init ids, learned entries first and a repeated id
-    // entering once, W * kBuf at a time) or a round of a step (at most G
-    // candidates per warp); the step's pick and its k update happen between
-    // rounds when the step's candidates are used up.
+    // Initial queue: the init ids (learned entries first, a repeated id
+    // entering once), W * kBuf at a time.
     const uint32_t *init = a.init_ids + (size_t) q * a.init_stride;
+    for (uint32_t r0 = 0; r0 < n_init; r0 += W * kBuf) {
+        uint32_t nb = 0;
+        const uint32_t lo = r0 + w * kBuf, hi = min(n_init, lo + kBuf);
+        for (uint32_t i0 = lo; i0 < hi; i0 += 32) {
+            const uint32_t i = i0 + lane;
+            const bool valid = i < hi;
+            const uint32_t id = valid ? (i < n_lrn ? cand[i] : __ldg(init + (i - n_lrn))) : 0u;
+            const bool ok = valid && id < a.n;
+            if (valid && !ok) atomicOr(a.error, ERR_BAD_INIT);
+            const uint32_t old = visit_issue(vis, id, ok);
+            note_dirty_block(ok && old == 0, id >> 5);
+            const bool fresh = ok && !(old & (1u << (id & 31)));
+            const uint32_t bm = __ballot_sync(kFull, fresh);
+            if (fresh) bi[nb + __popc(bm & lanemask_lt())] = id;
+            nb += __popc(bm);
+            __syncwarp();
+        }
+        finish_list(nb, false);
+        if (tid == 0) ctl[BC_NK] = L;
+        __syncthreads();
+        block_merge();
+    }
+
     uint32_t n_expand = 0, n_iter = 0;
     const uint32_t M = a.M;
     const uint32_t G = a.block_round;
-    bool in_init = true;
-    uint32_t r0 = 0, cnt = 0;
     for (;;) {
-        uint32_t nb = 0;
-        bool filter = true;
-        if (in_init && r0 >= n_init) {  // block-uniform
-            in_init = false;
-            r0 = 0;
-        }
-        if (in_init) {
-            const uint32_t lo = r0 + w * kBuf, hi = min(n_init, lo + kBuf);
-            for (uint32_t i0 = lo; i0 < hi; i0 += 32) {
-                const uint32_t i = i0 + lane;
-                const bool valid = i < hi;
-                const uint32_t id = valid ? (i < n_lrn ? cand[i] : __ldg(init + (i - n_lrn))) : 0u;
-                const bool ok = valid && id < a.n;
-                if (valid && !ok) atomicOr(a.error, ERR_BAD_INIT);
-                const uint32_t old = visit_issue(vis, id, ok);
-                note_dirty_block(ok && old == 0, id >> 5);
-                const bool fresh = ok && !(old & (1u << (id & 31)));
-                const uint32_t bm = __ballot_sync(kFull, fresh);
-                if (fresh) bi[nb + __popc(bm & lanemask_lt())] = id;
-                nb += __popc(bm);
+        // 1. Pick (warp 0), exactly as search_kernel.
+        if (w == 0) {
+            const uint32_t k = ctl[BC_K], sz = ctl[BC_SZ];
+            uint32_t cnt = 0, last_k = L;
+            for (uint32_t p0 = k; p0 < sz && cnt < M; p0 += 32) {
+                const uint32_t p = p0 + lane;
+                const bool un = p < sz && !(qi[p] & kChecked);
+                const uint32_t bm = __ballot_sync(kFull, un);
+                const uint32_t take = min((uint32_t) __popc(bm), M - cnt);
+                const uint32_t r = __popc(bm & lanemask_lt());
+                if (un && r < take) {
+                    const uint32_t id = qi[p];
+                    qi[p] = id | kChecked;
+                    cand[cnt + r] = id;
+                }
+                if (take) {
+                    uint32_t x = bm;
+                    for (uint32_t t = 1; t < take; ++t) x &= x - 1;
+                    last_k = p0 + (__ffs(x) - 1);
+                }
+                cnt += take;
                 __syncwarp();
             }
-            filter = false;
-            if (tid == 0) ctl[BC_NK] = L;
-            r0 += W * kBuf;
-        } else {
-            if (r0 >= cnt) {  // the step's candidates are used up (or none picked yet)
-                if (cnt) {
-                    if (tid == 0) {
-                        const uint32_t nk = ctl[BC_NK], last_k = ctl[BC_LASTK];
-                        ctl[BC_K] = nk <= last_k ? nk : last_k + 1;
-                    }
-                    __syncthreads();
-                }
-                // 1. Pick (warp 0), exactly as search_kernel.
-                if (w == 0) {
-                    const uint32_t k = ctl[BC_K], sz = ctl[BC_SZ];
-                    uint32_t cnt = 0, last_k = L;
-                    for (uint32_t p0 = k; p0 < sz && cnt < M; p0 += 32) {
-                        const uint32_t p = p0 + lane;
-                        const bool un = p < sz && !(qi[p] & kChecked);
-                        const uint32_t bm = __ballot_sync(kFull, un);
-                        const uint32_t take = min((uint32_t) __popc(bm), M - cnt);
-                        const uint32_t r = __popc(bm & lanemask_lt());
-                        if (un && r < take) {
-                            const uint32_t id = qi[p];
-                            qi[p] = id | kChecked;
-                            cand[cnt + r] = id;
-                        }
-                        if (take) {
-                            uint32_t x = bm;
-                            for (uint32_t t = 1; t < take; ++t) x &= x - 1;
-                            last_k = p0 + (__ffs(x) - 1);
-                        }
-                        cnt += take;
-                        __syncwarp();
-                    }
-                    if (lane == 0) {
-                        ctl[BC_CNT] = cnt;
-                        ctl[BC_LASTK] = last_k;
-                        ctl[BC_NK] = L;
-                    }
-                }
-                __syncthreads();
-                cnt = ctl[BC_CNT];
-                if (cnt == 0) break;
-                ++n_iter;
-                n_expand += cnt;
-                r0 = 0;
+            if (lane == 0) {
+                ctl[BC_CNT] = cnt;
+                ctl[BC_LASTK] = last_k;
+                ctl[BC_NK] = L;
             }
+        }
+        __syncthreads();
+        const uint32_t cnt = ctl[BC_CNT];
+        if (cnt == 0) break;
+        ++n_iter;
+        n_expand += cnt;
+        // 2-3. Rounds of at most G candidates per warp.
+        for (uint32_t r0 = 0; r0 < cnt; r0 += W * G) {
             // this warp's candidates: r0 + w + W * t, t < G
             uint32_t gc = 0;
             for (uint32_t t = 0; t < G; ++t)
                 if (r0 + w + W * t < cnt) ++gc;
-            nb = 0;
+            uint32_t nb = 0;
             if (gc) {
                 uint32_t hv[kCandGroup];
 #pragma unroll
@@ -378,11 +361,15 @@ __device__ void block_search_one(const SearchArgs &a, uint32_t q, uint8_t *smem,
                     }
                 }
             }
-            r0 += W * G;
+            finish_list(nb, true);
+            __syncthreads();
+            block_merge();
         }
-        finish_list(nb, filter);
+        if (tid == 0) {
+            const uint32_t nk = ctl[BC_NK], last_k = ctl[BC_LASTK];
+            ctl[BC_K] = nk <= last_k ? nk : last_k + 1;
+        }
         __syncthreads();
-        block_merge();
     }
 
     if constexpr (STORE != STORE_FP32) {
