@@ -340,7 +340,8 @@ def bench_ours(args):
             if store == N.STORE_FP32 and model is None:
                 continue
             c = AT.tune(handles[store], tune_q, tune_gt, K=K, target=TUNE_TARGET, storages=(store,), Ms=Ms,
-                        wpbs=(2, 4), learned_model=model, learned_opts=learned_opts if model is not None else (),
+                        wpbs=(2, 4), wpqs=(1, 2, 4, 8), learned_model=model,
+                        learned_opts=learned_opts if model is not None else (),
                         include_plain=store != N.STORE_FP32)
             cands.append(c)
         head = min(cands, key=lambda c: c.kernel_ms)
@@ -495,8 +496,9 @@ def bench_ours(args):
             with open(tp) as f:
                 entries = json.load(f)
             for tj in entries if isinstance(entries, list) else [entries]:
-                if (tj.get("L"), tj.get("M"), tj.get("n"), tj.get("storage"), tj.get("learned")) == (
-                        L, M, args.n, names[store], head.learned is not None):
+                if (tj.get("L"), tj.get("M"), tj.get("n"), tj.get("storage"), tj.get("learned"),
+                        tj.get("warps_per_query", 1)) == (L, M, args.n, names[store], head.learned is not None,
+                                                          head.warps_per_query):
                     traffic = tj["dram_bytes_per_query"] * nq
         except Exception:
             traffic = None

@@ -24,7 +24,7 @@ import numpy as np
 from . import native as N
 
 L_GRID = (100, 120, 140, 160, 180, 200, 224, 256, 288, 320, 352, 384, 416, 448, 512, 576, 640, 720, 800,
-          1024, 1280, 1600, 2048, 2560, 3072, 4096, 4608, 5120, 6144, 8192)
+          896, 1024, 1152, 1280, 1440, 1600, 1792, 2048, 2304, 2560, 3072, 4096, 4608, 5120, 6144, 8192)
 
 
 @dataclass
