@@ -21,6 +21,20 @@ def test_metric_names_follow_the_workload():
     assert b.metric_for(workloads.SPECS["mixture_1m_d96"]()) == b.METRIC
     assert "10M x 96d" in b.metric_for(workloads.SPECS["mixture_10m_d96"]())
     assert "1M x 128d" in b.metric_for(workloads.SPECS["u8_1m_d128"]())
+    assert "100M x 96d" in b.metric_for(workloads.SPECS["mixture_100m_d96"]())
+
+
+def test_large_workload_spec():
+    """The 100M configuration: 4,096 mixture components, R = 48, 10,000 cells
+    with 3 probed neighbours, reverse edges, one learned class per component,
+    held in memory; smaller bases scale the cell count (1 per 1,000 vectors)."""
+    from parallel_anns_b200 import workloads
+    s = workloads.SPECS["mixture_100m_d96"]()
+    assert (s["n"], s["d"], s["components"], s["R"], s["knn_k"]) == (100_000_000, 96, 4096, 48, 64)
+    assert (s["cells"], s["probe"], s["reverse"], s["reps"], s["large"]) == (10_000, 3, True, 4096, True)
+    assert workloads.SPECS["mixture_100m_d96"](n=2_000_000)["cells"] == 2000
+    b = load_bench()
+    assert b.TUNE_TARGET > b.RECALL_TARGET
 
 
 def test_host_workload_matches_store_and_load(tmp_path, monkeypatch):
