@@ -273,8 +273,9 @@ __device__ __forceinline__ uint32_t fresh_rank(const float *bd, const uint32_t *
 }
 
 // (dist, key) order of the fresh buffer: the key is the original vertex id
-// (PANNS) or the arrival index (EFANNA), distinct within a buffer, so the
-// order is total and needs no lookups.
+// or the device id (PANNS; then replaced by the original id when distances
+// tie, see flush) or the arrival index (EFANNA), distinct within a buffer, so
+// the order is total and needs no lookups.
 __device__ __forceinline__ bool plain_less(float ad, uint32_t ak, float bd, uint32_t bk) {
     return ad < bd || (ad == bd && ak < bk);
 }
@@ -733,6 +734,7 @@ static __device__ void rerank_output(float *qd, uint32_t *qi, uint32_t sz, uint3
 template <int KIND, int ORDER, int CL, int STORE>
 __device__ uint32_t flush(const SearchArgs &a, const WarpMem &m, uint32_t nb, uint32_t *sz, uint32_t L,
                           bool filter, const Dist<KIND, CL, STORE> &D, int lane) {
+    constexpr bool kLazyKeys = ORDER == ORDER_PANNS && STORE != STORE_FP8;
 #if PANNS_WIDE_DIST
     if constexpr (STORE == STORE_FP32) distances_wide<KIND, CL>(a, D.qv, m.bi, m.bd, nb, lane);
     else D.distances(a, m.bi, m.bd, nb, lane);
@@ -759,13 +761,28 @@ __device__ uint32_t flush(const SearchArgs &a, const WarpMem &m, uint32_t nb, ui
             const uint32_t pos = cnt + __popc(bm & lanemask_lt());
             m.bd[pos] = d;
             m.bi[pos] = id;
-            m.bk[pos] = ORDER == ORDER_PANNS ? __ldg(a.orig + id) : pos;
+            m.bk[pos] = ORDER == ORDER_PANNS ? (kLazyKeys ? id : __ldg(a.orig + id)) : pos;
         }
         cnt += __popc(bm);
         __syncwarp();
     }
     if (cnt == 0) return L;
-    warp_sort<ORDER>(m.bd, m.bi, m.bk, cnt, a.orig, lane);
+    // With lazy keys the survivors are sorted by (distance, device id); PANNS
+    // order breaks equal distances by original id, so if the sorted
+    // survivors hold equal distances (rare) they are sorted once more with
+    // the original ids as keys (one inlined copy of warp_sort either way).
+    // Measured (10,000 queries, L = 384, M = 8, same ids): float32 rows
+    // 5.42 -> 5.31 ms, BF16 5.08 -> 5.02 ms, FP8 5.03 -> 5.08 ms, so the FP8
+    // kernel keeps loading the original ids in the filter.
+    for (int pass = 0;; ++pass) {
+        warp_sort<ORDER>(m.bd, m.bi, m.bk, cnt, a.orig, lane);
+        if (!kLazyKeys || pass) break;
+        bool tie = false;
+        for (uint32_t i = lane; i + 1 < cnt; i += 32) tie |= m.bd[i] == m.bd[i + 1];
+        if (!__any_sync(kFull, tie)) break;
+        for (uint32_t i = lane; i < cnt; i += 32) m.bk[i] = __ldg(a.orig + (m.bi[i] & kIdMask));
+        __syncwarp();
+    }
     return warp_merge<ORDER>(m, sz, L, cnt, a.orig, lane);
 }
 
