@@ -1,5 +1,5 @@
 """The CPU oracle of the entry / L-budget network is itself pinned before it
-judges the GPU: its analytic gradient matches central differences of its own
+checks the GPU: its analytic gradient matches central differences of its own
 loss, its BF16 rounding matches known bit patterns (round to nearest, ties to
 even), and the per-query decision follows its stated rules."""
 import numpy as np
